@@ -1,0 +1,201 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes front-end of the CPU oracles.
+
+Loaded by the tests, by ``__graft_entry__.smoke()`` and by ``bench.py``'s
+CPU-baseline leg, as the checker.  Nothing in the product imports this module.
+
+* ``burn_f64``      -- FP64 restatement of the reference's Rust firelib
+                       (oracle/firelib_oracle.c)
+* ``burn_firelib_c``-- the reference's own C fireLib compiled from source
+                       (oracle/_ref/libfirelib_ref.so), driven like the
+                       reference's quickcheck harness
+* ``find_boundaries``, ``propagate``, ``post`` -- CPU restatement of the
+                       propagation kernel with the reference's tile schedule
+                       (oracle/propag_oracle.c)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIELDS = ("rx_int", "speed0", "hpua", "phi_eff_wind", "speed_max", "azimuth_max",
+          "eccentricity", "residence_time", "byrams_max", "flame_max")
+STAT_NAMES = ("rounds", "launches", "sweeps", "evaluations", "improvements", "gathers",
+              "dda_steps", "refbox_scans", "refbox_cells", "tiles_x", "tiles_y")
+
+_lib = None
+_ref = None
+
+
+def build(reference: str | None = None) -> None:
+    """Compiles liboracle.so and, when the reference checkout exists, _ref/."""
+    args = ["make", "-s", "-C", HERE, "all"]
+    subprocess.run(args, check=True)
+    ref_root = reference or "/root/reference"
+    if os.path.isdir(os.path.join(ref_root, "crates", "firelib-sys")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref_root}"], check=True)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _lib = C.CDLL(path)
+        f32p = C.POINTER(C.c_float)
+        _lib.ofl_burn_f64.restype = C.c_int64
+        _lib.ops_propagate.restype = C.c_int
+        _lib.ops_find_boundaries.restype = C.c_int64
+        _lib.ops_post.restype = C.c_int64
+        _lib.ops_post.argtypes = [C.c_int64, f32p, C.c_float, f32p]
+    return _lib
+
+
+def have_firelib_c() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libfirelib_ref.so"))
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(os.path.join(HERE, "_ref", "libfirelib_ref.so"))
+        _ref.ref_burn_c.restype = C.c_int64
+    return _ref
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+TERRAIN_KEYS = ("fuel_code", "d1hr", "d10hr", "d100hr", "herb", "wood",
+                "wind_speed", "wind_azimuth", "slope", "aspect")
+
+
+def _terrain_args(t):
+    fuel = np.ascontiguousarray(t["fuel_code"], dtype=np.uint8).ravel()
+    rest = [np.ascontiguousarray(t[k], dtype=np.float32).ravel() for k in TERRAIN_KEYS[1:]]
+    n = fuel.size
+    for r in rest:
+        assert r.size == n
+    return n, fuel, rest
+
+
+def burn_f64(terrain: dict) -> tuple[np.ndarray, np.ndarray]:
+    """Returns (fields[n, 10] float64, situation[n] int32)."""
+    lib = _load()
+    n, fuel, rest = _terrain_args(terrain)
+    out = np.zeros((n, 10), dtype=np.float64)
+    sit = np.zeros(n, dtype=np.int32)
+    lib.ofl_burn_f64(C.c_int64(n), _ptr(fuel), *[_ptr(r) for r in rest], _ptr(out), _ptr(sit))
+    return out, sit
+
+
+def burn_firelib_c(terrain: dict) -> np.ndarray:
+    lib = _load_ref()
+    n, fuel, rest = _terrain_args(terrain)
+    out = np.zeros((n, 10), dtype=np.float64)
+    lib.ref_burn_c(C.c_int64(n), _ptr(fuel), *[_ptr(r) for r in rest], _ptr(out))
+    return out
+
+
+def catalog_f64() -> np.ndarray:
+    lib = _load()
+    out = np.zeros((20, 17), dtype=np.float64)
+    lib.ofl_catalog_f64(_ptr(out), C.c_int(17))
+    return out
+
+
+class _Settings(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("dx", C.c_float),
+                ("dy", C.c_float), ("max_time", C.c_float)]
+
+
+def find_boundaries(width: int, height: int, speed, az, ecc) -> np.ndarray:
+    lib = _load()
+    n = width * height
+    bits = np.zeros((n + 31) // 32, dtype=np.uint32)
+    s, a, e = (np.ascontiguousarray(x, dtype=np.float32).ravel() for x in (speed, az, ecc))
+    lib.ops_find_boundaries(C.c_uint32(width), C.c_uint32(height), _ptr(s), _ptr(a), _ptr(e),
+                            _ptr(bits))
+    return bits
+
+
+@dataclass
+class OracleResult:
+    time: np.ndarray        # (H, W) float32 after the post mask
+    time_raw: np.ndarray    # (H, W) float32 before the post mask
+    refs_x: np.ndarray
+    refs_y: np.ndarray
+    boundaries: np.ndarray  # uint32 bit words
+    stats: dict
+
+
+def initial_state(width: int, height: int, ignitions):
+    """ignitions: iterable of (x, y, t).  Mirrors propag.rs:433-449: ignited
+    cells reference themselves, the rest hold 0xFFFF and f32::MAX."""
+    time = np.full(width * height, np.finfo(np.float32).max, dtype=np.float32)
+    rx = np.full(width * height, 0xFFFF, dtype=np.uint16)
+    ry = np.full(width * height, 0xFFFF, dtype=np.uint16)
+    for (x, y, t) in ignitions:
+        i = int(x) + int(y) * width
+        time[i] = np.float32(t)
+    ign = np.nonzero(time < np.finfo(np.float32).max)[0]
+    rx[ign] = (ign % width).astype(np.uint16)
+    ry[ign] = (ign // width).astype(np.uint16)
+    return time, rx, ry
+
+
+def propagate(width: int, height: int, dx: float, dy: float, max_time: float,
+              speed, az, ecc, ignitions=None, *, time0=None, refs0=None, tile: int = 0,
+              full: bool = False, trig: int = 0, threads: int = 0) -> OracleResult:
+    """Runs the CPU restatement.  tile = cells per side of one cooperative
+    launch (block * grid_w); 0 = one tile (global Jacobi)."""
+    lib = _load()
+    s_arr, a_arr, e_arr = (np.ascontiguousarray(x, dtype=np.float32).ravel() for x in (speed, az, ecc))
+    if time0 is None:
+        time, rx, ry = initial_state(width, height, ignitions or [])
+    else:
+        time = np.array(time0, dtype=np.float32).ravel().copy()
+        rx = np.array(refs0[0], dtype=np.uint16).ravel().copy()
+        ry = np.array(refs0[1], dtype=np.uint16).ravel().copy()
+    bits = find_boundaries(width, height, s_arr, a_arr, e_arr)
+    st = _Settings(width, height, dx, dy, max_time)
+    stats = np.zeros(len(STAT_NAMES), dtype=np.int64)
+    rc = lib.ops_propagate(C.byref(st), _ptr(s_arr), _ptr(a_arr), _ptr(e_arr), _ptr(time), _ptr(rx),
+                           _ptr(ry), _ptr(bits), C.c_int(tile), C.c_int(int(full)), C.c_int(trig),
+                           C.c_int(threads), _ptr(stats))
+    if rc != 0:
+        raise RuntimeError(f"ops_propagate failed: {rc}")
+    raw = time.copy()
+    lib.ops_post(C.c_int64(time.size), s_arr.ctypes.data_as(C.POINTER(C.c_float)),
+                 C.c_float(max_time), time.ctypes.data_as(C.POINTER(C.c_float)))
+    return OracleResult(time.reshape(height, width), raw.reshape(height, width),
+                        rx.reshape(height, width), ry.reshape(height, width), bits,
+                        dict(zip(STAT_NAMES, (int(v) for v in stats))))
+
+
+def time_from_batch(dx, dy, fx, fy, ftime, tx, ty, smax, azmax, ecc, trig=0):
+    lib = _load()
+    st = _Settings(0, 0, dx, dy, 0.0)
+    arrs = [np.ascontiguousarray(a, dtype=t) for a, t in
+            ((fx, np.int32), (fy, np.int32), (ftime, np.float32), (tx, np.int32), (ty, np.int32),
+             (smax, np.float32), (azmax, np.float32), (ecc, np.float32))]
+    n = arrs[0].size
+    out = np.zeros(n, dtype=np.float32)
+    lib.ops_time_from_batch(C.byref(st), C.c_int64(n), *[_ptr(a) for a in arrs], C.c_int(trig), _ptr(out))
+    return out
+
+
+def trig_batch(a, b):
+    lib = _load()
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    b = np.ascontiguousarray(b, dtype=np.float32)
+    c = np.zeros_like(a)
+    t = np.zeros_like(a)
+    lib.ops_trig_batch(C.c_int64(a.size), _ptr(a), _ptr(b), _ptr(c), _ptr(t))
+    return c, t
