@@ -1,0 +1,202 @@
+/*
+ * propag_b200.h -- B200 entry points of libpropag.so beyond the reference ABI.
+ *
+ * Plain C: pointers, sizes and an opaque stream handle (a cudaStream_t passed
+ * as void*).  Every function returns PROPAG_OK (0) or a negative status; the
+ * message of the last failure on the calling thread is propag_last_error().
+ * There is no CPU fallback: without a usable CUDA device every compute entry
+ * point fails with PROPAG_ERR_NO_DEVICE.
+ *
+ * The computations are the reference's hot path (paths relative to the
+ * reference project):
+ *   fire behaviour   crates/firelib/src/cuda.rs:9-95 (cuda_standard_burn,
+ *                    cuda_standard_simple_burn) over firelib.rs:996-1188
+ *   propagation      crates/propag/src/propag.cu (pre_propagate, propag,
+ *                    post_propagate) driven as crates/propag/src/propag.rs:392-556
+ */
+#ifndef PROPAG_B200_H
+#define PROPAG_B200_H
+
+#include "propag_host.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PROPAG_OK 0
+#define PROPAG_ERR_INVALID (-1)   /* bad argument */
+#define PROPAG_ERR_CUDA (-2)      /* a CUDA call failed */
+#define PROPAG_ERR_NO_DEVICE (-3) /* no CUDA device */
+#define PROPAG_ERR_TIMEOUT (-4)   /* a bounded device-side wait gave up */
+#define PROPAG_ERR_OOM (-5)       /* device memory exhausted */
+#define PROPAG_ERR_LOADER (-6)    /* the terrain loader callback returned false */
+
+/* Cells per side of one super-grid tile when a caller asks for the default.
+ * The reference launches one cooperative grid of w x w blocks of 19 x 19
+ * threads per tile, w = floor(sqrt(SMs * max active blocks per SM))
+ * (crates/propag/src/propag.rs:392-418); on a 148-SM B200 with two resident
+ * blocks per SM that is 17 blocks, 323 cells. */
+#define PROPAG_DEFAULT_TILE 323
+#define PROPAG_TILE_WHOLE_GRID (-1)
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *propag_last_error(void);
+
+/* Number of CUDA devices visible (0 when there is none or no driver). */
+int propag_device_count(void);
+
+/* Version string of this library. */
+const char *propag_version(void);
+
+/* Terrain structure-of-arrays, FFITerrain order (crates/propag/src/propag.rs:
+ * 763-775).  Host or device pointers depending on the entry point. */
+typedef struct PropagTerrainPtrs {
+  const uint8_t *fuel_code;
+  const float *d1hr;
+  const float *d10hr;
+  const float *d100hr;
+  const float *herb;
+  const float *wood;
+  const float *wind_speed;
+  const float *wind_azimuth;
+  const float *slope;
+  const float *aspect;
+} PropagTerrainPtrs;
+
+/* The ten per-cell fire fields, SI units: crates/firelib/src/cuda.rs:20-27
+ * (FireCuda) plus Byram's intensity (W/m) and flame length (m) of
+ * crates/firelib/src/firelib.rs:424-441.  A NULL pointer skips that field. */
+typedef struct PropagFireFields {
+  float *rx_int;         /* W/m^2 */
+  float *speed0;         /* m/s   */
+  float *hpua;           /* J/m^2 */
+  float *phi_eff_wind;   /* -     */
+  float *speed_max;      /* m/s   */
+  float *azimuth_max;    /* rad   */
+  float *eccentricity;   /* -     */
+  float *residence_time; /* s     */
+  float *byrams_max;     /* W/m   */
+  float *flame_max;      /* m     */
+} PropagFireFields;
+
+/* Fire behaviour of n cells, device pointers, stream-ordered (no sync).
+ * Cells without fire (fuel 0 or >= 14) get 0 in every field, as the
+ * reference's zero-initialised outputs hold (crates/propag/src/propag.rs:437-439).
+ * Replaces cuda_standard_simple_burn, crates/firelib/src/cuda.rs:57-95. */
+int propag_fire_simple_device(uint64_t n, const PropagTerrainPtrs *terrain, float *speed_max,
+                              float *azimuth_max, float *eccentricity, void *stream);
+
+/* All fields (the FireCuda fields written by cuda_standard_burn,
+ * crates/firelib/src/cuda.rs:7-55, plus Byram and flame). */
+int propag_fire_full_device(uint64_t n, const PropagTerrainPtrs *terrain,
+                            const PropagFireFields *out, void *stream);
+
+/* Same over host buffers: copies in, runs, copies out, synchronises. */
+int propag_fire_simple_host(uint64_t n, const PropagTerrainPtrs *terrain, float *speed_max,
+                            float *azimuth_max, float *eccentricity);
+int propag_fire_full_host(uint64_t n, const PropagTerrainPtrs *terrain,
+                          const PropagFireFields *out);
+
+/* One ignited cell (the result of rasterising a TimeFeature). */
+typedef struct PropagIgnition {
+  uint32_t x;
+  uint32_t y;
+  float time;
+} PropagIgnition;
+
+typedef struct PropagOptions {
+  int32_t tile;    /* default super-grid tile side; 0 = PROPAG_DEFAULT_TILE,
+                      PROPAG_TILE_WHOLE_GRID = one tile for the whole grid */
+  int32_t cluster; /* CTAs (one cluster) cooperating on one scenario, 1..16; 0 = auto */
+  int32_t threads; /* threads per CTA, multiple of 32, <= 512; 0 = 512 */
+  int32_t device;  /* CUDA device ordinal; -1 = the current device */
+} PropagOptions;
+
+typedef struct PropagStats {
+  uint64_t rounds;       /* passes over all tiles (propag.rs:502-536) */
+  uint64_t launches;     /* tile launches (one cooperative launch each in the reference) */
+  uint64_t sweeps;       /* Jacobi sweeps summed over launches */
+  uint64_t evaluations;  /* cells evaluated (find_neighbor_which_reaches_first) */
+  uint64_t improvements; /* cells whose time improved (commit_point) */
+  uint64_t dda_steps;    /* cells visited by line-of-sight walks */
+  uint64_t refbox_scans; /* changed cells that were some cell's reference */
+  uint64_t burned;       /* cells with time < FLT_MAX after the post mask */
+  uint64_t gathers;      /* time[reference] reads (burning neighbours with a reference) */
+  /* SM cycles the cluster leader spent per phase, barrier waits included:
+   * first sweeps of tile launches, evaluate, commit, referrer scans */
+  uint64_t cyc_first, cyc_eval, cyc_commit, cyc_scan;
+  uint32_t status;       /* 0 ok; nonzero: device-side error code */
+  uint32_t max_walk;     /* longest line-of-sight walk (cells) */
+} PropagStats;
+
+/* One scenario of a batch.  All pointers are device pointers; time, refs and
+ * boundaries are outputs.  dy < 0 means a north-up transform (propag.cu:274). */
+typedef struct PropagJob {
+  uint32_t width;
+  uint32_t height;
+  float dx;
+  float dy;
+  float max_time;
+  int32_t tile; /* 0 = the engine's default */
+  const float *speed_max;
+  const float *azimuth_max;
+  const float *eccentricity;
+  const PropagIgnition *ignitions;
+  uint32_t n_ignitions;
+  uint32_t pad;
+  float *time;          /* arrival time, s; FLT_MAX = not burned (post_propagate mask) */
+  uint16_t *refs_x;     /* reference cell of each burned cell (0xFFFF: none) */
+  uint16_t *refs_y;
+  uint32_t *boundaries; /* ceil(width*height/32) words, bit i = cell i is a boundary */
+} PropagJob;
+
+/* The batched propagation engine.  It owns the scratch memory of the
+ * propagation (work lists, reference boxes) and reuses it across calls. */
+typedef struct propag_engine propag_engine;
+
+propag_engine *propag_engine_create(const PropagOptions *opt);
+void propag_engine_destroy(propag_engine *engine);
+
+/* Propagates n_jobs scenarios in one persistent launch.  Stream-ordered; the
+ * call returns once the work is enqueued unless stats is non-NULL, in which
+ * case it synchronises and fills stats[n_jobs]. */
+int propag_engine_run(propag_engine *engine, const PropagJob *jobs, uint32_t n_jobs, void *stream,
+                      PropagStats *stats);
+
+/* Device time of the last propag_engine_run's kernels, from CUDA events
+ * recorded on its stream around each launch: ms[0] boundary/initial-state
+ * pass + ignition scatter, ms[1] propagation kernel, ms[2] post mask.
+ * Waits for the last run to finish. */
+int propag_engine_last_times(propag_engine *engine, float ms[3]);
+
+/* Plain drop-in over host buffers for one grid: fire behaviour (3 fields),
+ * boundaries, propagation and post mask, like propagate()
+ * (crates/propag/src/propag.rs:323-574) without the file writers.
+ * time (W*H), refs_x/refs_y (W*H) and boundaries (ceil(W*H/32)) are host
+ * outputs; refs/boundaries may be NULL. */
+int propag_run_host(const Settings *settings, const PropagTerrainPtrs *terrain,
+                    const PropagIgnition *ignitions, uint64_t n_ignitions,
+                    const PropagOptions *opt, float *time, uint16_t *refs_x, uint16_t *refs_y,
+                    uint32_t *boundaries, PropagStats *stats);
+
+/* Rasterises TimeFeatures (WKB Point, MultiPoint, LineString, Polygon and
+ * their Multi forms; Z/M ignored) onto the grid the way GDALRasterizeGeometries
+ * burns them (crates/propag/src/propag.rs:837-890): the cell containing a
+ * point, every cell a line passes through, every cell whose centre lies inside
+ * a polygon; later features overwrite earlier ones.  Features with invalid
+ * WKB are skipped, as the reference's filter_map does (propag.rs:213-215).
+ * Writes at most max_out ignitions; returns the number of ignited cells
+ * (< 0 on error). */
+int64_t propag_rasterize_ignitions(const GeoReference *geo_ref, const FFITimeFeature *features,
+                                   uint64_t n_features, PropagIgnition *out, uint64_t max_out);
+
+/* Writes width*height arrival times as a single-band float32 GeoTIFF, tiled
+ * 256 x 256, with the geo transform and nodata f32::MAX, as write_times does
+ * (crates/propag/src/propag.rs:576-600). */
+int propag_write_geotiff(const GeoReference *geo_ref, const float *time, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PROPAG_B200_H */

@@ -360,6 +360,7 @@ static int burn_cell(uint8_t code, const float in[9], double out[OFL_NFIELDS]) {
     pew = f->wind_k * pow(max_wind, f->wind_b);
     ew = max_wind;
     smax = speed0 * (1.0 + pew);
+    situation += 10; /* reported: the wind limit applied */
   }
   /* eccentricity, :1171-1174 */
   const double lw = 1.0 + 0.002840909 * ew;

@@ -1,0 +1,868 @@
+// extern "C" surface of libpropag.so: the reference plugin ABI
+// (include/propag_host.h) and the B200 entry points (include/propag_b200.h).
+//
+// Host orchestration follows propagate() (crates/propag/src/propag.rs:323-574):
+// terrain -> fire behaviour -> boundaries -> propagation -> post mask ->
+// outputs.  All device work is stream-ordered; nothing here computes fire
+// behaviour or arrival times on the CPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "engine.cuh"
+#include "io.hpp"
+#include "propag_b200.h"
+
+namespace propag {
+
+// launchers (fire.cu, engine_launch.cu)
+cudaError_t upload_catalog();
+cudaError_t launch_fire(bool full, uint64_t n, const uint8_t *fuel, const float *const m[5],
+                        const float *ws, const float *waz, const float *slope,
+                        const float *aspect, float *const outs[10], int sm_count,
+                        cudaStream_t stream);
+cudaError_t launch_prep(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
+                        cudaStream_t stream);
+cudaError_t launch_ignite(const JobDev *jobs, uint32_t n_jobs, cudaStream_t stream);
+cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
+                          uint32_t n_slots, int csize, int threads, uint32_t *queue,
+                          StatsDev *stats, unsigned long long max_sweeps, cudaStream_t stream);
+cudaError_t engine_max_clusters(int csize, int threads, int *n);
+cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
+                        StatsDev *stats, cudaStream_t stream);
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(e == cudaErrorMemoryAllocation ? PROPAG_ERR_OOM : PROPAG_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+struct DeviceState {
+  bool ready = false;
+  int sms = 0;
+};
+std::mutex g_dev_mu;
+DeviceState g_dev[64];
+
+// Selects the device (opt device or current), uploads the fuel table once per
+// device.  Fails loudly when there is no device: there is no CPU path.
+int ensure_device(int want, int *sms_out) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(PROPAG_ERR_NO_DEVICE, "no CUDA device available (libpropag has no CPU path)");
+  }
+  int dev = want;
+  if (dev < 0) CK(cudaGetDevice(&dev));
+  if (dev >= count || dev >= 64) return fail(PROPAG_ERR_INVALID, "device ordinal out of range");
+  CK(cudaSetDevice(dev));
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  DeviceState &d = g_dev[dev];
+  if (!d.ready) {
+    CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(upload_catalog());
+    d.ready = true;
+  }
+  if (sms_out) *sms_out = d.sms;
+  return PROPAG_OK;
+}
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  // Grows to at least `bytes`.  Growth waits for `stream` first.
+  cudaError_t reserve(size_t bytes, cudaStream_t stream) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) {
+      cudaError_t e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) return e;
+      cudaFree(p);
+      p = nullptr;
+      cap = 0;
+    }
+    const size_t want = bytes + bytes / 8 + 256;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) return e;
+    cap = want;
+    return cudaSuccess;
+  }
+  template <typename T>
+  T *at(size_t off) const {
+    return reinterpret_cast<T *>(static_cast<char *>(p) + off);
+  }
+};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+bool valid_size(uint32_t w, uint32_t h) { return w >= 1 && h >= 1 && w <= 65534 && h <= 65534; }
+
+}  // namespace
+}  // namespace propag
+
+using namespace propag;
+
+// ============================================================ engine ======
+struct propag_engine {
+  int device = 0;
+  int sms = 0;
+  int csize = 0;    // 0 = auto
+  int threads = 512;  // the engine kernel's launch bound
+  int default_tile = PROPAG_DEFAULT_TILE;
+  cudaStream_t stream = nullptr;  // the stream of the last run
+  DevBuf job_scratch, slot_scratch, meta;
+  JobDev *jobs_pinned = nullptr;
+  SlotDev *slots_pinned = nullptr;
+  size_t pinned_jobs = 0, pinned_slots = 0;
+  cudaEvent_t staged = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around prep, engine, post
+};
+
+extern "C" propag_engine *propag_engine_create(const PropagOptions *opt) {
+  int sms = 0;
+  const int want = opt ? opt->device : -1;
+  if (ensure_device(want, &sms) != PROPAG_OK) return nullptr;
+  auto *e = new propag_engine();
+  cudaGetDevice(&e->device);
+  e->sms = sms;
+  if (opt) {
+    if (opt->cluster < 0 || opt->cluster > 16) {
+      fail(PROPAG_ERR_INVALID, "cluster must be 0..16");
+      delete e;
+      return nullptr;
+    }
+    e->csize = opt->cluster;
+    if (opt->threads) {
+      if (opt->threads % 32 || opt->threads > 512) {
+        fail(PROPAG_ERR_INVALID, "threads must be a multiple of 32, <= 512");
+        delete e;
+        return nullptr;
+      }
+      e->threads = opt->threads;
+    }
+    if (opt->tile) e->default_tile = opt->tile;
+  }
+  bool ok = cudaEventCreateWithFlags(&e->staged, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < 4; ++i) ok = ok && cudaEventCreate(&e->ev[i]) == cudaSuccess;
+  if (!ok) {
+    fail(PROPAG_ERR_CUDA, "cudaEventCreate failed");
+    delete e;
+    return nullptr;
+  }
+  return e;
+}
+
+extern "C" void propag_engine_destroy(propag_engine *e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->staged) {
+    cudaEventSynchronize(e->staged);
+    cudaEventDestroy(e->staged);
+  }
+  for (int i = 0; i < 4; ++i)
+    if (e->ev[i]) cudaEventDestroy(e->ev[i]);
+  if (e->jobs_pinned) cudaFreeHost(e->jobs_pinned);
+  if (e->slots_pinned) cudaFreeHost(e->slots_pinned);
+  delete e;
+}
+
+static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, cudaStream_t stream,
+                      PropagStats *stats) {
+  if (!e) return fail(PROPAG_ERR_INVALID, "null engine");
+  if (n_jobs == 0) return PROPAG_OK;
+  if (!jobs) return fail(PROPAG_ERR_INVALID, "null jobs");
+  CK(cudaSetDevice(e->device));
+  // ---- validate and lay out per-job scratch ----
+  std::vector<JobDev> jd(n_jobs);
+  std::vector<size_t> off(n_jobs);
+  size_t job_bytes = 0, tn_max = 1;
+  uint64_t max_cells = 1;
+  for (uint32_t i = 0; i < n_jobs; ++i) {
+    const PropagJob &j = jobs[i];
+    if (!valid_size(j.width, j.height))
+      return fail(PROPAG_ERR_INVALID, "job " + std::to_string(i) + ": width/height must be 1..65534");
+    if (!j.speed_max || !j.azimuth_max || !j.eccentricity || !j.time)
+      return fail(PROPAG_ERR_INVALID, "job " + std::to_string(i) + ": null fire/time pointer");
+    if (j.n_ignitions && !j.ignitions)
+      return fail(PROPAG_ERR_INVALID, "job " + std::to_string(i) + ": null ignitions");
+    if (!(j.dx != 0.0f) || !(j.dy != 0.0f) || !std::isfinite(j.dx) || !std::isfinite(j.dy))
+      return fail(PROPAG_ERR_INVALID, "job " + std::to_string(i) + ": invalid pixel size");
+    const uint64_t N = (uint64_t)j.width * j.height;
+    const uint64_t words = (N + 31) / 32;
+    int T = j.tile ? j.tile : e->default_tile;
+    if (T == PROPAG_TILE_WHOLE_GRID || T <= 0) T = (int)std::max(j.width, j.height);
+    JobDev &d = jd[i];
+    d.W = (int)j.width;
+    d.H = (int)j.height;
+    d.gdx = j.dx;
+    d.gdy = j.dy;
+    d.max_time = j.max_time;
+    d.T = T;
+    d.TX = (int)((j.width + T - 1) / T);
+    d.TY = (int)((j.height + T - 1) / T);
+    d.north_up = j.dy < 0 ? 1 : 0;
+    d.speed = j.speed_max;
+    d.az = j.azimuth_max;
+    d.ecc = j.eccentricity;
+    d.time = j.time;
+    d.ignitions = j.ignitions;
+    d.n_ignitions = j.n_ignitions;
+    d.out_rx = j.refs_x;
+    d.out_ry = j.refs_y;
+    d.out_bnd = j.boundaries;
+    off[i] = job_bytes;
+    job_bytes += align_up(N * 4, 256) * 3 + (j.boundaries ? 0 : align_up(words * 4, 256));
+    tn_max = std::max<size_t>(tn_max, (size_t)std::min<uint32_t>(T, j.width) * std::min<uint32_t>(T, j.height));
+    max_cells = std::max<uint64_t>(max_cells, N);
+  }
+  CK(e->job_scratch.reserve(job_bytes, stream));
+  for (uint32_t i = 0; i < n_jobs; ++i) {
+    const uint64_t N = (uint64_t)jd[i].W * jd[i].H;
+    size_t o = off[i];
+    jd[i].refs = e->job_scratch.at<uint32_t>(o);
+    o += align_up(N * 4, 256);
+    jd[i].box_lo = e->job_scratch.at<uint32_t>(o);
+    o += align_up(N * 4, 256);
+    jd[i].box_hi = e->job_scratch.at<uint32_t>(o);
+    o += align_up(N * 4, 256);
+    jd[i].bnd = jobs[i].boundaries ? jobs[i].boundaries : e->job_scratch.at<uint32_t>(o);
+  }
+  // ---- cluster slots ----
+  int csize = e->csize;
+  int max_clusters = 0;
+  if (csize == 0) {
+    // enough clusters for every job, as large as the machine allows
+    int per_sm = 0;
+    CK(engine_max_clusters(1, e->threads, &per_sm));  // = resident CTAs
+    const int ctas = std::max(per_sm, 1);
+    csize = 1;
+    while (csize < 16 && (uint64_t)(csize * 2) * n_jobs <= (uint64_t)ctas) csize *= 2;
+  }
+  CK(engine_max_clusters(csize, e->threads, &max_clusters));
+  if (max_clusters < 1) return fail(PROPAG_ERR_CUDA, "cluster size " + std::to_string(csize) + " cannot be resident");
+  const uint32_t n_slots = std::min<uint32_t>(n_jobs, (uint32_t)max_clusters);
+  const size_t words_max = tn_max / 32 + 1;
+  const size_t slot_bytes = align_up(tn_max * 4, 256) * 3 + align_up(words_max * 4, 256) +
+                            align_up(tn_max * sizeof(Update), 256) + 256;
+  CK(e->slot_scratch.reserve(slot_bytes * n_slots, stream));
+  // meta: jobs, slots, stats, queue
+  const size_t meta_jobs = align_up(sizeof(JobDev) * n_jobs, 256);
+  const size_t meta_slots = align_up(sizeof(SlotDev) * n_slots, 256);
+  const size_t meta_stats = align_up(sizeof(StatsDev) * n_jobs, 256);
+  CK(e->meta.reserve(meta_jobs + meta_slots + meta_stats + 256, stream));
+  // staging buffers (pinned) may still be read by the previous run's copies
+  CK(cudaEventSynchronize(e->staged));
+  if (e->pinned_jobs < n_jobs) {
+    if (e->jobs_pinned) cudaFreeHost(e->jobs_pinned);
+    CK(cudaMallocHost(&e->jobs_pinned, sizeof(JobDev) * n_jobs));
+    e->pinned_jobs = n_jobs;
+  }
+  if (e->pinned_slots < n_slots) {
+    if (e->slots_pinned) cudaFreeHost(e->slots_pinned);
+    CK(cudaMallocHost(&e->slots_pinned, sizeof(SlotDev) * n_slots));
+    e->pinned_slots = n_slots;
+  }
+  std::copy(jd.begin(), jd.end(), e->jobs_pinned);
+  for (uint32_t s = 0; s < n_slots; ++s) {
+    size_t o = slot_bytes * s;
+    SlotDev &sd = e->slots_pinned[s];
+    sd.cand[0] = e->slot_scratch.at<uint32_t>(o);
+    o += align_up(tn_max * 4, 256);
+    sd.cand[1] = e->slot_scratch.at<uint32_t>(o);
+    o += align_up(tn_max * 4, 256);
+    sd.scan = e->slot_scratch.at<uint32_t>(o);
+    o += align_up(tn_max * 4, 256);
+    sd.dirty = e->slot_scratch.at<uint32_t>(o);
+    o += align_up(words_max * 4, 256);
+    sd.upd = e->slot_scratch.at<Update>(o);
+    o += align_up(tn_max * sizeof(Update), 256);
+    sd.ctr = e->slot_scratch.at<uint32_t>(o);
+    // the dirty bitmap and counters must start cleared
+    CK(cudaMemsetAsync(sd.dirty, 0, words_max * 4, stream));
+    CK(cudaMemsetAsync(sd.ctr, 0, 64, stream));
+  }
+  JobDev *d_jobs = e->meta.at<JobDev>(0);
+  SlotDev *d_slots = e->meta.at<SlotDev>(meta_jobs);
+  StatsDev *d_stats = e->meta.at<StatsDev>(meta_jobs + meta_slots);
+  uint32_t *d_queue = e->meta.at<uint32_t>(meta_jobs + meta_slots + meta_stats);
+  CK(cudaMemcpyAsync(d_jobs, e->jobs_pinned, sizeof(JobDev) * n_jobs, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_slots, e->slots_pinned, sizeof(SlotDev) * n_slots, cudaMemcpyHostToDevice, stream));
+  CK(cudaEventRecord(e->staged, stream));
+  CK(cudaMemsetAsync(d_stats, 0, sizeof(StatsDev) * n_jobs, stream));
+  CK(cudaMemsetAsync(d_queue, 0, 4, stream));
+  // ---- kernels ----
+  CK(cudaEventRecord(e->ev[0], stream));
+  CK(launch_prep(d_jobs, n_jobs, max_cells, e->sms, stream));
+  CK(launch_ignite(d_jobs, n_jobs, stream));
+  CK(cudaEventRecord(e->ev[1], stream));
+  CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, d_queue, d_stats,
+                   1ull << 40, stream));
+  CK(cudaEventRecord(e->ev[2], stream));
+  CK(launch_post(d_jobs, n_jobs, max_cells, e->sms, d_stats, stream));
+  CK(cudaEventRecord(e->ev[3], stream));
+  e->stream = stream;
+  if (stats) {
+    std::vector<StatsDev> hs(n_jobs);
+    CK(cudaMemcpyAsync(hs.data(), d_stats, sizeof(StatsDev) * n_jobs, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    for (uint32_t i = 0; i < n_jobs; ++i) {
+      PropagStats &o = stats[i];
+      o.rounds = hs[i].rounds;
+      o.launches = hs[i].launches;
+      o.sweeps = hs[i].sweeps;
+      o.evaluations = hs[i].evaluations;
+      o.improvements = hs[i].improvements;
+      o.dda_steps = hs[i].dda_steps;
+      o.gathers = hs[i].gathers;
+      o.refbox_scans = hs[i].refbox_scans;
+      o.burned = hs[i].burned;
+      o.cyc_first = hs[i].cyc_first;
+      o.cyc_eval = hs[i].cyc_eval;
+      o.cyc_commit = hs[i].cyc_commit;
+      o.cyc_scan = hs[i].cyc_scan;
+      o.status = hs[i].status;
+      o.max_walk = hs[i].max_walk;
+    }
+    for (uint32_t i = 0; i < n_jobs; ++i)
+      if (hs[i].status) return fail(PROPAG_ERR_TIMEOUT, "job " + std::to_string(i) + ": sweep limit reached");
+  }
+  return PROPAG_OK;
+}
+
+extern "C" int propag_engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs,
+                                 void *stream, PropagStats *stats) {
+  return engine_run(e, jobs, n_jobs, (cudaStream_t)stream, stats);
+}
+
+extern "C" int propag_engine_last_times(propag_engine *e, float ms[3]) {
+  if (!e || !ms) return fail(PROPAG_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(e->device));
+  CK(cudaEventSynchronize(e->ev[3]));
+  for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms[i], e->ev[i], e->ev[i + 1]));
+  return PROPAG_OK;
+}
+
+// ======================================================== fire behaviour ==
+static int fire_device(bool full, uint64_t n, const PropagTerrainPtrs *t, float *const outs[10],
+                       cudaStream_t stream) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (!t) return fail(PROPAG_ERR_INVALID, "null terrain");
+  if (n == 0) return PROPAG_OK;
+  if (!t->fuel_code || !t->d1hr || !t->d10hr || !t->d100hr || !t->herb || !t->wood ||
+      !t->wind_speed || !t->wind_azimuth || !t->slope || !t->aspect)
+    return fail(PROPAG_ERR_INVALID, "null terrain raster");
+  const float *m[5] = {t->d1hr, t->d10hr, t->d100hr, t->herb, t->wood};
+  CK(launch_fire(full, n, t->fuel_code, m, t->wind_speed, t->wind_azimuth, t->slope, t->aspect,
+                 outs, sms, stream));
+  return PROPAG_OK;
+}
+
+extern "C" int propag_fire_simple_device(uint64_t n, const PropagTerrainPtrs *terrain,
+                                         float *speed_max, float *azimuth_max,
+                                         float *eccentricity, void *stream) {
+  float *outs[10] = {nullptr, nullptr, nullptr, nullptr, speed_max, azimuth_max, eccentricity,
+                     nullptr, nullptr, nullptr};
+  return fire_device(false, n, terrain, outs, (cudaStream_t)stream);
+}
+
+extern "C" int propag_fire_full_device(uint64_t n, const PropagTerrainPtrs *terrain,
+                                       const PropagFireFields *o, void *stream) {
+  if (!o) return fail(PROPAG_ERR_INVALID, "null outputs");
+  float *outs[10] = {o->rx_int, o->speed0, o->hpua, o->phi_eff_wind, o->speed_max,
+                     o->azimuth_max, o->eccentricity, o->residence_time, o->byrams_max,
+                     o->flame_max};
+  return fire_device(true, n, terrain, outs, (cudaStream_t)stream);
+}
+
+namespace {
+// Device copies of a host terrain (+ outputs) for the host-buffer entry points.
+struct HostPath {
+  DevBuf buf;
+  std::mutex mu;
+};
+HostPath &host_path() {
+  static HostPath hp;
+  return hp;
+}
+
+int upload_terrain(DevBuf &buf, uint64_t n, const PropagTerrainPtrs *t, size_t extra,
+                   PropagTerrainPtrs *dev, cudaStream_t s) {
+  const size_t fb = align_up(n, 256), ff = align_up(n * 4, 256);
+  CK(buf.reserve(fb + 9 * ff + extra, s));
+  uint8_t *fuel = buf.at<uint8_t>(0);
+  float *f[9];
+  for (int k = 0; k < 9; ++k) f[k] = buf.at<float>(fb + k * ff);
+  const float *src[9] = {t->d1hr, t->d10hr, t->d100hr, t->herb, t->wood,
+                         t->wind_speed, t->wind_azimuth, t->slope, t->aspect};
+  CK(cudaMemcpyAsync(fuel, t->fuel_code, n, cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < 9; ++k) CK(cudaMemcpyAsync(f[k], src[k], n * 4, cudaMemcpyHostToDevice, s));
+  *dev = PropagTerrainPtrs{fuel, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8]};
+  return PROPAG_OK;
+}
+}  // namespace
+
+static int fire_host(bool full, uint64_t n, const PropagTerrainPtrs *t, float *const host_outs[10]) {
+  int rc = ensure_device(-1, nullptr);
+  if (rc) return rc;
+  if (!t) return fail(PROPAG_ERR_INVALID, "null terrain");
+  if (n == 0) return PROPAG_OK;
+  HostPath &hp = host_path();
+  std::lock_guard<std::mutex> lk(hp.mu);
+  cudaStream_t s = 0;
+  const size_t base = align_up(n, 256) + 9 * align_up(n * 4, 256);
+  PropagTerrainPtrs dev{};
+  rc = upload_terrain(hp.buf, n, t, 10 * align_up(n * 4, 256), &dev, s);
+  if (rc) return rc;
+  float *douts[10];
+  for (int k = 0; k < 10; ++k) douts[k] = host_outs[k] ? hp.buf.at<float>(base + k * align_up(n * 4, 256)) : nullptr;
+  rc = fire_device(full, n, &dev, douts, s);
+  if (rc) return rc;
+  for (int k = 0; k < 10; ++k)
+    if (host_outs[k]) CK(cudaMemcpyAsync(host_outs[k], douts[k], n * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return PROPAG_OK;
+}
+
+extern "C" int propag_fire_simple_host(uint64_t n, const PropagTerrainPtrs *terrain,
+                                       float *speed_max, float *azimuth_max, float *eccentricity) {
+  float *outs[10] = {nullptr, nullptr, nullptr, nullptr, speed_max, azimuth_max, eccentricity,
+                     nullptr, nullptr, nullptr};
+  return fire_host(false, n, terrain, outs);
+}
+
+extern "C" int propag_fire_full_host(uint64_t n, const PropagTerrainPtrs *terrain,
+                                     const PropagFireFields *o) {
+  if (!o) return fail(PROPAG_ERR_INVALID, "null outputs");
+  float *outs[10] = {o->rx_int, o->speed0, o->hpua, o->phi_eff_wind, o->speed_max,
+                     o->azimuth_max, o->eccentricity, o->residence_time, o->byrams_max,
+                     o->flame_max};
+  return fire_host(true, n, terrain, outs);
+}
+
+// ======================================================= plain drop-in ====
+namespace {
+struct RunHostState {
+  std::mutex mu;
+  propag_engine *engine = nullptr;
+  int engine_tile = 0, engine_cluster = -1, engine_threads = -1, engine_device = -2;
+  DevBuf buf;
+};
+RunHostState &run_state() {
+  static RunHostState s;
+  return s;
+}
+}  // namespace
+
+extern "C" int propag_run_host(const Settings *settings, const PropagTerrainPtrs *terrain,
+                               const PropagIgnition *ignitions, uint64_t n_ignitions,
+                               const PropagOptions *opt, float *time, uint16_t *refs_x,
+                               uint16_t *refs_y, uint32_t *boundaries, PropagStats *stats) {
+  if (!settings || !terrain || !time) return fail(PROPAG_ERR_INVALID, "null argument");
+  const GeoReference &g = settings->geo_ref;
+  if (!valid_size(g.width, g.height)) return fail(PROPAG_ERR_INVALID, "width/height must be 1..65534");
+  if (n_ignitions && !ignitions) return fail(PROPAG_ERR_INVALID, "null ignitions");
+  int rc = ensure_device(opt ? opt->device : -1, nullptr);
+  if (rc) return rc;
+  RunHostState &st = run_state();
+  std::lock_guard<std::mutex> lk(st.mu);
+  PropagOptions o = opt ? *opt : PropagOptions{0, 0, 0, -1};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (!st.engine || st.engine_tile != o.tile || st.engine_cluster != o.cluster ||
+      st.engine_threads != o.threads || st.engine_device != dev) {
+    if (st.engine) propag_engine_destroy(st.engine);
+    st.engine = propag_engine_create(&o);
+    if (!st.engine) return PROPAG_ERR_INVALID;
+    st.engine_tile = o.tile;
+    st.engine_cluster = o.cluster;
+    st.engine_threads = o.threads;
+    st.engine_device = dev;
+  }
+  cudaStream_t s = 0;
+  const uint64_t N = (uint64_t)g.width * g.height;
+  const uint64_t words = (N + 31) / 32;
+  const size_t tb = align_up(N, 256) + 9 * align_up(N * 4, 256);
+  const size_t ff = align_up(N * 4, 256);
+  const size_t extra = 4 * ff + 2 * align_up(N * 2, 256) + align_up(words * 4, 256) +
+                       align_up(n_ignitions * sizeof(PropagIgnition) + 16, 256);
+  PropagTerrainPtrs dev_t{};
+  rc = upload_terrain(st.buf, N, terrain, extra, &dev_t, s);
+  if (rc) return rc;
+  size_t o2 = tb;
+  float *d_speed = st.buf.at<float>(o2); o2 += ff;
+  float *d_az = st.buf.at<float>(o2); o2 += ff;
+  float *d_ecc = st.buf.at<float>(o2); o2 += ff;
+  float *d_time = st.buf.at<float>(o2); o2 += ff;
+  uint16_t *d_rx = st.buf.at<uint16_t>(o2); o2 += align_up(N * 2, 256);
+  uint16_t *d_ry = st.buf.at<uint16_t>(o2); o2 += align_up(N * 2, 256);
+  uint32_t *d_bnd = st.buf.at<uint32_t>(o2); o2 += align_up(words * 4, 256);
+  PropagIgnition *d_ign = st.buf.at<PropagIgnition>(o2);
+  if (n_ignitions)
+    CK(cudaMemcpyAsync(d_ign, ignitions, n_ignitions * sizeof(PropagIgnition), cudaMemcpyHostToDevice, s));
+  rc = propag_fire_simple_device(N, &dev_t, d_speed, d_az, d_ecc, s);
+  if (rc) return rc;
+  PropagJob job{};
+  job.width = g.width;
+  job.height = g.height;
+  job.dx = g.transform.gt.dx;
+  job.dy = g.transform.gt.dy;
+  job.max_time = settings->max_time;
+  job.tile = 0;
+  job.speed_max = d_speed;
+  job.azimuth_max = d_az;
+  job.eccentricity = d_ecc;
+  job.ignitions = d_ign;
+  job.n_ignitions = (uint32_t)n_ignitions;
+  job.time = d_time;
+  job.refs_x = d_rx;
+  job.refs_y = d_ry;
+  job.boundaries = d_bnd;
+  PropagStats js{};
+  rc = engine_run(st.engine, &job, 1, s, &js);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(time, d_time, N * 4, cudaMemcpyDeviceToHost, s));
+  if (refs_x) CK(cudaMemcpyAsync(refs_x, d_rx, N * 2, cudaMemcpyDeviceToHost, s));
+  if (refs_y) CK(cudaMemcpyAsync(refs_y, d_ry, N * 2, cudaMemcpyDeviceToHost, s));
+  if (boundaries) CK(cudaMemcpyAsync(boundaries, d_bnd, words * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (stats) *stats = js;
+  return PROPAG_OK;
+}
+
+// ====================================================== rasterisation ====
+extern "C" int64_t propag_rasterize_ignitions(const GeoReference *g, const FFITimeFeature *f,
+                                              uint64_t n, PropagIgnition *out, uint64_t max_out) {
+  if (!g) return fail(PROPAG_ERR_INVALID, "null geo_ref");
+  if (n && !f) return fail(PROPAG_ERR_INVALID, "null features");
+  int64_t k = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (!f[i].geom_wkb || f[i].geom_wkb_len == 0) continue;  // propag.rs:130-141
+    Geometry geom;
+    if (!parse_wkb(f[i].geom_wkb, f[i].geom_wkb_len, geom)) continue;
+    const float t = f[i].time;
+    rasterize(*g, geom, [&](int64_t c, int64_t r) {
+      if ((uint64_t)k < max_out && out) out[k] = PropagIgnition{(uint32_t)c, (uint32_t)r, t};
+      ++k;
+    });
+  }
+  return k;
+}
+
+extern "C" int propag_write_geotiff(const GeoReference *g, const float *time, const char *path) {
+  if (!g || !time || !path) return fail(PROPAG_ERR_INVALID, "null argument");
+  std::string err;
+  if (!write_geotiff_f32(path, *g, time, err)) return fail(PROPAG_ERR_INVALID, err);
+  return PROPAG_OK;
+}
+
+// ========================================================= misc ===========
+extern "C" const char *propag_last_error(void) { return g_error.c_str(); }
+
+extern "C" int propag_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+extern "C" const char *propag_version(void) { return "propag-b200 0.1.0 (sm_100a)"; }
+
+// ======================================================= plugin ABI =======
+extern "C" Settings create_settings(GeoReference geo_ref, float max_time) {
+  Settings s;
+  s.geo_ref = geo_ref;
+  s.max_time = max_time;
+  return s;
+}
+
+extern "C" FireSimpleCuda create_fire(float speed_max, float azimuth_max, float eccentricity) {
+  return FireSimpleCuda{speed_max, azimuth_max, eccentricity};
+}
+
+extern "C" uint32_t GeoReference_len(const GeoReference *g) { return g->width * g->height; }
+extern "C" float GeoReference_x0(const GeoReference *g) {
+  const GT &t = g->transform.gt;
+  return t.dx > 0.0f ? t.x0 : t.x0 + t.dx * (float)g->width;
+}
+extern "C" float GeoReference_x1(const GeoReference *g) {
+  const GT &t = g->transform.gt;
+  return t.dx > 0.0f ? t.x0 + t.dx * (float)g->width : t.x0;
+}
+extern "C" float GeoReference_y0(const GeoReference *g) {
+  const GT &t = g->transform.gt;
+  return t.dy > 0.0f ? t.y0 : t.y0 + t.dy * (float)g->height;
+}
+extern "C" float GeoReference_y1(const GeoReference *g) {
+  const GT &t = g->transform.gt;
+  return t.dy > 0.0f ? t.y0 + t.dy * (float)g->height : t.y0;
+}
+
+// GT::invert, crates/geometry/src/lib.rs:84-124 (f32 arithmetic).
+static bool gt_invert(const GT &a, GT &inv) {
+  if (a.rx == 0.0f && a.ry == 0.0f && a.dx != 0.0f && a.dy != 0.0f) {
+    inv = GT{-a.x0 / a.dx, 1.0f / a.dx, 0.0f, -a.y0 / a.dy, 0.0f, 1.0f / a.dy};
+    return true;
+  }
+  const float det = a.dx * a.dy - a.rx * a.ry;
+  const float mag = std::max(std::max(std::fabs(a.dx), std::fabs(a.rx)),
+                             std::max(std::fabs(a.ry), std::fabs(a.dy)));
+  if (!(std::fabs(det) > 1e-10f * mag * mag)) return false;
+  const float id = 1.0f / det;
+  inv = GT{(a.rx * a.y0 - a.x0 * a.dy) * id, a.dy * id, -a.rx * id,
+           (-a.dx * a.y0 + a.x0 * a.ry) * id, -a.ry * id, a.dx * id};
+  return true;
+}
+
+// NumCast f32 -> u32 (fails on NaN, negative, too large).
+static bool to_u32(float v, uint32_t &out) {
+  if (!(v >= 0.0f) || !(v < 4294967296.0f)) return false;
+  out = (uint32_t)v;
+  return true;
+}
+
+// GeoReference::south_up / north_up, crates/geometry/src/lib.rs:239-276.
+static bool make_georef(bool north, float x0, float y0, float x1, float y1, float dx, float dy,
+                        const char *proj, GeoReference *result) {
+  if (!proj || !result) return false;
+  const size_t len = strlen(proj);
+  if (len >= sizeof(result->proj)) return false;
+  GeoReference g;
+  std::memset(&g, 0, sizeof(g));
+  g.transform.gt = north ? GT{x0, dx, 0.0f, y1, 0.0f, -dy} : GT{x0, dx, 0.0f, y0, 0.0f, dy};
+  if (!gt_invert(g.transform.gt, g.transform.inv)) return false;
+  if (!to_u32(std::ceil((x1 - x0) / dx), g.width)) return false;
+  if (!to_u32(std::ceil((y1 - y0) / dy), g.height)) return false;
+  std::memcpy(g.proj, proj, len);
+  *result = g;
+  return true;
+}
+
+extern "C" bool GeoReference_south_up(float x0, float y0, float x1, float y1, float dx, float dy,
+                                      const char *proj, GeoReference *result) {
+  return make_georef(false, x0, y0, x1, y1, dx, dy, proj, result);
+}
+extern "C" bool GeoReference_north_up(float x0, float y0, float x1, float y1, float dx, float dy,
+                                      const char *proj, GeoReference *result) {
+  return make_georef(true, x0, y0, x1, y1, dx, dy, proj, result);
+}
+
+static void copy_err(char *err_msg, uintptr_t err_len, const std::string &msg) {
+  if (err_msg && err_len) strncpy(err_msg, msg.c_str(), err_len);  // propag.rs:295-306
+}
+
+static std::string norm_crs(const char *s) {
+  std::string out;
+  bool space = false;
+  for (const char *p = s; *p; ++p) {
+    if (*p == ' ' || *p == '\t' || *p == '\n') {
+      space = !out.empty();
+      continue;
+    }
+    if (space) out.push_back(' ');
+    space = false;
+    out.push_back(*p);
+  }
+  return out;
+}
+
+extern "C" bool propag_rasterize_fuels(const FFIFuelFeature *fuels, uintptr_t fuels_len,
+                                       const char *fuels_crs, const GeoReference *geo_ref,
+                                       uint8_t *result, char *err_msg, uintptr_t err_len) {
+  if (!geo_ref || !result) {
+    copy_err(err_msg, err_len, "null geo_ref or result");
+    return false;
+  }
+  if (!fuels_crs) {
+    copy_err(err_msg, err_len, "invalid fuels CRS");
+    return false;
+  }
+  const std::string grid = norm_crs((const char *)geo_ref->proj), src = norm_crs(fuels_crs);
+  if (!src.empty() && src != grid) {
+    copy_err(err_msg, err_len,
+             "fuels CRS differs from the grid CRS; this build does not reproject (pass geometries in the grid CRS)");
+    return false;
+  }
+  const uint64_t N = (uint64_t)geo_ref->width * geo_ref->height;
+  std::memset(result, 255, N);  // nodata (propag.rs:941-943)
+  for (uintptr_t i = 0; fuels && i < fuels_len; ++i) {
+    if (!fuels[i].geom_wkb || fuels[i].geom_wkb_len == 0) continue;
+    Geometry geom;
+    if (!parse_wkb(fuels[i].geom_wkb, fuels[i].geom_wkb_len, geom)) continue;
+    const uint8_t code = fuels[i].code;
+    rasterize(*geo_ref, geom, [&](int64_t c, int64_t r) { result[c + r * (int64_t)geo_ref->width] = code; });
+  }
+  return true;
+}
+
+// Writes one WKT geometry per line as CSV (GDAL reads it with the CSV driver);
+// stands in for the reference's GPKG layers (propag.rs:601-750).
+static bool write_wkt_csv(const std::string &path, const std::vector<std::string> &rows,
+                          std::string &err) {
+  FILE *f = std::fopen(path.c_str(), "w");
+  if (!f) {
+    err = "cannot open " + path;
+    return false;
+  }
+  std::fputs("WKT\n", f);
+  for (const std::string &r : rows) {
+    std::fputc('"', f);
+    std::fputs(r.c_str(), f);
+    std::fputs("\"\n", f);
+  }
+  return std::fclose(f) == 0;
+}
+
+static std::string pt_str(const GeoReference &g, double c, double r) {
+  const GT &t = g.transform.gt;
+  const double x = (double)t.x0 + c * (double)t.dx + r * (double)t.rx;
+  const double y = (double)t.y0 + c * (double)t.ry + r * (double)t.dy;
+  char b[96];
+  std::snprintf(b, sizeof(b), "%.9g %.9g", x, y);
+  return b;
+}
+
+static std::string rect_wkt(const GeoReference &g, double c0, double r0, double c1, double r1) {
+  return "POLYGON((" + pt_str(g, c0, r0) + ", " + pt_str(g, c1, r0) + ", " + pt_str(g, c1, r1) +
+         ", " + pt_str(g, c0, r1) + ", " + pt_str(g, c0, r0) + "))";
+}
+
+extern "C" bool FFIPropagation_run(FFIPropagation p, uintptr_t err_len, char *err_msg) {
+  try {
+    const GeoReference &g = p.settings.geo_ref;
+    if (!p.output_path || !*p.output_path) {
+      copy_err(err_msg, err_len, "invalid output_path");
+      return false;
+    }
+    if (!valid_size(g.width, g.height)) {
+      copy_err(err_msg, err_len, "grid width/height must be 1..65534");
+      return false;
+    }
+    if (!p.initial_ignited_elements_crs) {
+      copy_err(err_msg, err_len, "invalid initial_ignited_elements_crs");
+      return false;
+    }
+    const std::string grid = norm_crs((const char *)g.proj), src = norm_crs(p.initial_ignited_elements_crs);
+    if (!src.empty() && src != grid) {
+      copy_err(err_msg, err_len,
+               "ignition CRS differs from the grid CRS; this build does not reproject (pass geometries in the grid CRS)");
+      return false;
+    }
+    // ignitions (invalid WKB silently dropped, propag.rs:213-215)
+    std::vector<PropagIgnition> ign;
+    const uint64_t nf = p.initial_ignited_elements ? p.initial_ignited_elements_len : 0;
+    const int64_t k = propag_rasterize_ignitions(&g, p.initial_ignited_elements, nf, nullptr, 0);
+    if (k < 0) {
+      copy_err(err_msg, err_len, g_error);
+      return false;
+    }
+    ign.resize((size_t)k);
+    propag_rasterize_ignitions(&g, p.initial_ignited_elements, nf, ign.data(), ign.size());
+    // terrain through the callback (FFITerrainLoader::load_extent, propag.rs:813-835)
+    const uint64_t N = (uint64_t)g.width * g.height;
+    std::vector<uint8_t> fuel(N, 0);
+    std::vector<std::vector<float>> fl(9, std::vector<float>(N, 0.0f));
+    FFITerrain t{fuel.data(), fl[0].data(), fl[1].data(), fl[2].data(), fl[3].data(),
+                 fl[4].data(), fl[5].data(), fl[6].data(), fl[7].data(), fl[8].data()};
+    if (!p.terrain_loader.load || !p.terrain_loader.load(p.terrain_loader.context, &g, &t)) {
+      copy_err(err_msg, err_len, "load_extent_error");
+      return false;
+    }
+    PropagTerrainPtrs tp{fuel.data(), fl[0].data(), fl[1].data(), fl[2].data(), fl[3].data(),
+                         fl[4].data(), fl[5].data(), fl[6].data(), fl[7].data(), fl[8].data()};
+    std::vector<float> time(N);
+    std::vector<uint16_t> rx(N), ry(N);
+    std::vector<uint32_t> bnd((N + 31) / 32);
+    PropagStats stats{};
+    const int rc = propag_run_host(&p.settings, &tp, ign.data(), ign.size(), nullptr, time.data(),
+                                   rx.data(), ry.data(), bnd.data(), &stats);
+    if (rc) {
+      copy_err(err_msg, err_len, g_error);
+      return false;
+    }
+    std::string err;
+    if (!write_geotiff_f32(p.output_path, g, time.data(), err)) {
+      copy_err(err_msg, err_len, err);
+      return false;
+    }
+    if (p.refs_output_path && *p.refs_output_path) {  // write_refs, propag.rs:699-750
+      std::vector<std::string> rows;
+      for (uint32_t i = 0; i < g.width; ++i)
+        for (uint32_t j = 0; j < g.height; ++j) {
+          const uint64_t ix = i + (uint64_t)j * g.width;
+          if (time[ix] < FLT_MAX)
+            rows.push_back("LINESTRING(" + pt_str(g, rx[ix] + 0.5, ry[ix] + 0.5) + ", " +
+                           pt_str(g, i + 0.5, j + 0.5) + ")");
+        }
+      if (!write_wkt_csv(p.refs_output_path, rows, err)) {
+        copy_err(err_msg, err_len, err);
+        return false;
+      }
+    }
+    // tile outlines (write_boundaries, propag.rs:601-697): the "grid" layer is
+    // the super-grid tile, the "block" layer its 19 x 19 thread blocks
+    const bool want_grid = p.grid_boundaries_out_path && *p.grid_boundaries_out_path;
+    const bool want_block = p.block_boundaries_out_path && *p.block_boundaries_out_path;
+    if (want_grid || want_block) {
+      const uint32_t T = PROPAG_DEFAULT_TILE, B = 19;
+      const uint32_t sx = (g.width + T - 1) / T, sy = (g.height + T - 1) / T;
+      std::vector<std::string> grids, blocks;
+      for (uint32_t gy = 0; gy < sy; ++gy)
+        for (uint32_t gx = 0; gx < sx; ++gx) {
+          grids.push_back(rect_wkt(g, gx * T, gy * T, (gx + 1) * T, (gy + 1) * T));
+          for (uint32_t by = 0; by < T / B; ++by)
+            for (uint32_t bx = 0; bx < T / B; ++bx)
+              blocks.push_back(rect_wkt(g, gx * T + bx * B, gy * T + by * B, gx * T + (bx + 1) * B,
+                                        gy * T + (by + 1) * B));
+        }
+      if (want_grid && !write_wkt_csv(p.grid_boundaries_out_path, grids, err)) {
+        copy_err(err_msg, err_len, err);
+        return false;
+      }
+      if (want_block && !write_wkt_csv(p.block_boundaries_out_path, blocks, err)) {
+        copy_err(err_msg, err_len, err);
+        return false;
+      }
+    }
+    return true;
+  } catch (const std::exception &ex) {  // catch_unwind, propag.rs:280-308
+    copy_err(err_msg, err_len, ex.what());
+    return false;
+  } catch (...) {
+    copy_err(err_msg, err_len, "unknown error");
+    return false;
+  }
+}
+
+extern "C" PluginT create_plugin(void) {
+  PluginT p;
+  p.run = FFIPropagation_run;
+  p.rasterize_fuels = propag_rasterize_fuels;
+  return p;
+}

@@ -1,0 +1,320 @@
+// Per-cell fire behaviour (Rothermel / BEHAVE) as an elementwise FP32 pass
+// over structure-of-arrays rasters.
+//
+// Reference (paths relative to the reference project):
+//   cuda_standard_simple_burn / cuda_standard_burn   crates/firelib/src/cuda.rs:7-95
+//   Fuel::burn / burn_simple                         crates/firelib/src/firelib.rs:996-1030
+//   rx_int_rbqig, eta_m                              firelib.rs:1031-1076
+//   calculate_wind_dependent_vars, situations        firelib.rs:1078-1167
+//   eccentricity, phi_slope, phi_wind                firelib.rs:1171-1188
+//   Terrain::upslope                                 firelib.rs:400-409
+//   Byram's intensity, flame length                  firelib.rs:424-441
+//
+// Layout and mapping: every thread handles 4 consecutive cells with 128-bit
+// loads of each of the nine float rasters and one 32-bit load of the fuel
+// codes, and 128-bit stores of each output; the grid is a multiple of the SM
+// count and strides over the rasters.  The fuel table sits in shared memory
+// (14 models x 40 floats), indexed per cell.
+//
+// FP32 formulation.  The arithmetic is the reference's, rearranged where the
+// float evaluation of the literal formula loses accuracy against double:
+//   * the moisture sums are pre-folded per moisture class; the dead and live
+//     sums and the live extinction moisture are double-float (error-free
+//     products and sums), because they are subtracted from the moisture of
+//     extinction, where float cancellation would dominate the error;
+//   * eta_m = 1 - 2.59 rt + 5.11 rt^2 - 3.52 rt^3 is evaluated in
+//     u = 1 - rt = (mext - moist) / mext as u (2.93 - 5.45 u + 3.52 u^2),
+//     the same cubic expanded at rt = 1 where it vanishes;
+//   * the cross-slope direction uses atan2(|y|, |x|) instead of
+//     asin(|y| / hypot(x, y)) (same angle, no loss near 90 degrees);
+//   * the cross-slope vector is summed in phi units (the reference's rate
+//     vectors divided by speed0 > 0), so phi_ew2 is its length instead of
+//     (speed0 + rv) / speed0 - 1;
+//   * eccentricity sqrt(lw^2 - 1) / lw with lw = 1 + a is sqrt(a (2 + a)) / (1 + a);
+//   * pi and 2 pi are added as float pairs (hi + lo).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "catalog.hpp"
+
+namespace propag {
+
+constexpr float kSmidgenF = 1e-6f;  // SMIDGEN, crates/firelib/src/f32.rs:5
+constexpr float kPiHi = 3.14159274101257324f, kPiLo = -8.74227766e-8f;
+constexpr float kTwoPiHi = 6.28318548202514648f, kTwoPiLo = -1.74845553e-7f;
+// unit conversions (crates/firelib/src/units.rs:28-30: foot 0.3048 m,
+// BTU 1054.35 J)
+constexpr float kFpmToMps = 0.00508f;             // 0.3048 / 60
+constexpr float kMpsToFpm = 196.850393700787402f; // 60 / 0.3048
+constexpr float kRxToSI = 189.146876418865f;      // BTU/ft^2/min -> W/m^2
+constexpr float kHpuaToSI = 11348.8125851319f;    // BTU/ft^2 -> J/m^2
+constexpr float kByramsToSI = 3459.15354330709f;  // BTU/ft/s -> W/m
+constexpr float kFootToM = 0.3048f;
+
+__constant__ FuelConst c_catalog[kMaxFuels];
+
+struct FireOut {
+  float rx_int, speed0, hpua, phi_eff_wind, speed_max, azimuth_max, eccentricity,
+      residence_time, byrams, flame;
+};
+
+// Double-float value hi + lo (|lo| <= ulp(hi) / 2).
+struct DF {
+  float hi, lo;
+};
+
+// Error-free sum of two floats (Knuth's two-sum).
+__device__ __forceinline__ DF two_sum(float a, float b) {
+  const float s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  const float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return DF{s, e};
+}
+
+// sum_k (chi[k] + clo[k]) * m[k] as a double-float: exact products (fma) and
+// sums (two-sum), so that moisture sums keep ~2^-44 relative accuracy.
+__device__ __forceinline__ DF dot5_df(const float *chi, const float *clo, const float m[5]) {
+  float hi = 0.0f, lo = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const float p = __fmul_rn(chi[k], m[k]);
+    const float pe = __fmaf_rn(chi[k], m[k], -p);
+    const DF s = two_sum(hi, p);
+    hi = s.hi;
+    lo = __fadd_rn(lo, __fadd_rn(s.lo, __fmaf_rn(clo[k], m[k], pe)));
+  }
+  return two_sum(hi, lo);
+}
+
+__device__ __forceinline__ DF df_sub(DF a, DF b) {
+  const DF s = two_sum(a.hi, -b.hi);
+  return two_sum(s.hi, __fadd_rn(s.lo, __fsub_rn(a.lo, b.lo)));
+}
+
+// eta_m (firelib.rs:1060-1076) with rt = moist / mext, as
+// u (2.93 - 5.45 u + 3.52 u^2), u = 1 - rt = (mext - moist) / mext.
+__device__ __forceinline__ float eta_m(DF moist, DF mext) {
+  const DF d = df_sub(mext, moist);
+  if (!(d.hi > 0.0f)) return 0.0f;  // life_moist >= life_mext
+  const float u = __fdiv_rn(d.hi + d.lo, mext.hi + mext.lo);
+  return u * fmaf(u, fmaf(u, 3.52f, -5.45f), 2.93f);
+}
+
+__device__ __forceinline__ float dot5(const float *c, const float m[5]) {
+  float s = c[0] * m[0];
+  s = fmaf(c[1], m[1], s);
+  s = fmaf(c[2], m[2], s);
+  s = fmaf(c[3], m[3], s);
+  return fmaf(c[4], m[4], s);
+}
+
+__device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], float ws,
+                                          float waz, float slope, float aspect, FireOut &o) {
+  // rx_int_rbqig
+  const DF dead = dot5_df(F.A, F.A_lo, m);
+  const DF live = dot5_df(F.B, F.B_lo, m);
+  const float rbqig = F.R0 + dot5(F.R, m);
+  const DF mext{F.mext, F.mext_lo};
+  const float eta_dead = eta_m(dead, mext);
+  DF live_mext{0.0f, 0.0f};
+  if (F.has_live != 0.0f) {
+    live_mext = df_sub(DF{F.LM0, F.LM0_lo}, dot5_df(F.LM, F.LM_lo, m));
+    if (!(df_sub(live_mext, mext).hi > 0.0f)) live_mext = mext;  // max(live_mext, mext)
+  }
+  const float eta_live = eta_m(live, live_mext);
+  const float rx = fmaf(F.rx_alive, eta_live, F.rx_dead * eta_dead);
+  const float speed0 = __fdiv_rn(rx * F.flux_ratio, rbqig);
+
+  // calculate_wind_dependent_vars
+  const float phi_slope = F.slope_k * slope * slope;
+  const float ws_fpm = ws * kMpsToFpm;
+  const float phi_wind = F.wind_k * powf(ws_fpm, F.wind_b);
+  const float phi_ew = phi_slope + phi_wind;
+  const float upslope = aspect >= kPiHi ? (aspect - kPiHi) - kPiLo : (aspect + kPiHi) + kPiLo;
+  const float max_wind = 0.9f * rx;
+
+  float pew = phi_ew, ew = 0.0f, smax = 0.0f, az = 0.0f;
+  bool limit = true;
+  if (speed0 < kSmidgenF) {  // NoSpread
+    limit = false;
+  } else if (phi_ew < kSmidgenF) {  // NoSlopeNoWind
+    smax = speed0;
+    limit = false;
+  } else if (slope < kSmidgenF) {  // WindNoSlope
+    ew = ws_fpm;
+    smax = speed0 * (1.0f + phi_ew);
+    az = waz;
+  } else if (ws < kSmidgenF || fabsf(upslope - waz) < kSmidgenF) {  // SlopeNoWind, UpSlope
+    ew = powf(phi_ew * F.wind_e, F.wind_b_inv);
+    smax = speed0 * (1.0f + phi_ew);
+    az = upslope;
+  } else {  // CrossSlope
+    // The reference sums the rate vectors speed0 * phi; the common factor
+    // speed0 > 0 is kept out: (x, y) below are those vectors / speed0, the
+    // direction and quadrant are unchanged and phi_ew2 = |(x, y)|.
+    const float split = upslope <= waz ? waz - upslope : ((kTwoPiHi - upslope) + waz) + kTwoPiLo;
+    float sn, cs;
+    sincosf(split, &sn, &cs);
+    const float x = fmaf(phi_wind, cs, phi_slope);
+    const float y = phi_wind * sn;
+    pew = hypotf(x, y);
+    smax = speed0 * (1.0f + pew);
+    ew = powf(pew * F.wind_e, F.wind_b_inv);
+    const float al = atan2f(fabsf(y), fabsf(x));
+    float split2;
+    if (x >= 0.0f && y >= 0.0f) split2 = al;
+    else if (x >= 0.0f) split2 = (kTwoPiHi - al) + kTwoPiLo;
+    else if (y >= 0.0f) split2 = (kPiHi - al) + kPiLo;
+    else split2 = (kPiHi + al) + kPiLo;
+    az = upslope + split2;
+    if (az > kTwoPiHi) az = (az - kTwoPiHi) - kTwoPiLo;
+  }
+  if (limit && ew > max_wind) {  // check_wind_limit
+    pew = F.wind_k * powf(max_wind, F.wind_b);
+    ew = max_wind;
+    smax = speed0 * (1.0f + pew);
+  }
+  const float a = 0.002840909f * ew;
+  o.speed_max = smax * kFpmToMps;
+  o.azimuth_max = az;
+  o.eccentricity = __fdiv_rn(sqrtf(a * (2.0f + a)), 1.0f + a);
+  {  // the remaining FireCuda fields, Byram and flame
+    o.rx_int = rx * kRxToSI;
+    o.speed0 = speed0 * kFpmToMps;
+    o.hpua = rx * F.residence_time * kHpuaToSI;
+    o.phi_eff_wind = pew;
+    o.residence_time = F.residence_time * 60.0f;
+    const float byrams = F.residence_time * smax * rx * (1.0f / 60.0f);
+    o.byrams = byrams * kByramsToSI;
+    o.flame = byrams > kSmidgenF ? 0.45f * powf(byrams, 0.46f) * kFootToM : 0.0f;
+  }
+}
+
+struct Inputs {
+  const uint8_t *fuel;
+  const float *m[5];
+  const float *ws, *waz, *slope, *aspect;
+};
+struct Outputs {
+  float *f[10];  // PropagFireFields order
+};
+
+__device__ __forceinline__ void store_cell(const Outputs &out, uint64_t i, const FireOut &o) {
+  const float v[10] = {o.rx_int, o.speed0, o.hpua, o.phi_eff_wind, o.speed_max,
+                       o.azimuth_max, o.eccentricity, o.residence_time, o.byrams, o.flame};
+#pragma unroll
+  for (int k = 0; k < 10; ++k)
+    if (out.f[k]) out.f[k][i] = v[k];
+}
+
+__device__ __forceinline__ void one_cell(const FuelConst *cat, const Inputs &in, const Outputs &out,
+                                         uint64_t i) {
+  const uint8_t code = in.fuel[i];
+  FireOut o{};
+  if (code < kMaxFuels && cat[code].has_fire != 0.0f) {
+    const float m[5] = {in.m[0][i], in.m[1][i], in.m[2][i], in.m[3][i], in.m[4][i]};
+    burn_cell(cat[code], m, in.ws[i], in.waz[i], in.slope[i], in.aspect[i], o);
+  }
+  store_cell(out, i, o);
+}
+
+// Vector path: all pointers 16-byte aligned; cells [0, n4*4) in groups of 4.
+__global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, uint64_t n) {
+  __shared__ FuelConst cat[kMaxFuels];
+  for (int t = threadIdx.x; t < (int)(sizeof(cat) / 4); t += blockDim.x)
+    reinterpret_cast<float *>(cat)[t] = reinterpret_cast<const float *>(c_catalog)[t];
+  __syncthreads();
+  const uint64_t n4 = n / 4;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n4; g += stride) {
+    const uchar4 fc = __ldg(reinterpret_cast<const uchar4 *>(in.fuel) + g);
+    float4 mv[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) mv[k] = __ldg(reinterpret_cast<const float4 *>(in.m[k]) + g);
+    const float4 ws = __ldg(reinterpret_cast<const float4 *>(in.ws) + g);
+    const float4 wa = __ldg(reinterpret_cast<const float4 *>(in.waz) + g);
+    const float4 sl = __ldg(reinterpret_cast<const float4 *>(in.slope) + g);
+    const float4 as = __ldg(reinterpret_cast<const float4 *>(in.aspect) + g);
+    const uint8_t codes[4] = {fc.x, fc.y, fc.z, fc.w};
+    FireOut o[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      o[c] = FireOut{};
+      const uint8_t code = codes[c];
+      if (code < kMaxFuels && cat[code].has_fire != 0.0f) {
+        const float m[5] = {(&mv[0].x)[c], (&mv[1].x)[c], (&mv[2].x)[c], (&mv[3].x)[c],
+                            (&mv[4].x)[c]};
+        burn_cell(cat[code], m, (&ws.x)[c], (&wa.x)[c], (&sl.x)[c], (&as.x)[c], o[c]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      if (!out.f[k]) continue;
+      float4 v;
+      float *vp = &v.x;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float vv[10] = {o[c].rx_int, o[c].speed0, o[c].hpua, o[c].phi_eff_wind,
+                              o[c].speed_max, o[c].azimuth_max, o[c].eccentricity,
+                              o[c].residence_time, o[c].byrams, o[c].flame};
+        vp[c] = vv[k];
+      }
+      reinterpret_cast<float4 *>(out.f[k])[g] = v;
+    }
+  }
+  // tail
+  const uint64_t t0 = n4 * 4;
+  for (uint64_t i = t0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    one_cell(cat, in, out, i);
+}
+
+// Scalar path for unaligned pointers.
+__global__ void __launch_bounds__(256) fire_kernel_scalar(Inputs in, Outputs out, uint64_t n) {
+  __shared__ FuelConst cat[kMaxFuels];
+  for (int t = threadIdx.x; t < (int)(sizeof(cat) / 4); t += blockDim.x)
+    reinterpret_cast<float *>(cat)[t] = reinterpret_cast<const float *>(c_catalog)[t];
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    one_cell(cat, in, out, i);
+}
+
+// ---- host-side launchers (called from api.cpp) ------------------------------
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+cudaError_t upload_catalog() {
+  FuelConst table[kMaxFuels];
+  build_catalog_table(table);
+  return cudaMemcpyToSymbol(c_catalog, table, sizeof(table));
+}
+
+cudaError_t launch_fire(bool full, uint64_t n, const uint8_t *fuel, const float *const m[5],
+                        const float *ws, const float *waz, const float *slope,
+                        const float *aspect, float *const outs[10], int sm_count,
+                        cudaStream_t stream) {
+  Inputs in{fuel, {m[0], m[1], m[2], m[3], m[4]}, ws, waz, slope, aspect};
+  Outputs out{};
+  bool aligned = ((uintptr_t)fuel & 3u) == 0;
+  for (int k = 0; k < 5; ++k) aligned = aligned && aligned16(m[k]);
+  aligned = aligned && aligned16(ws) && aligned16(waz) && aligned16(slope) && aligned16(aspect);
+  for (int k = 0; k < 10; ++k) {
+    out.f[k] = outs[k];
+    if (outs[k]) aligned = aligned && aligned16(outs[k]);
+  }
+  if (n == 0) return cudaSuccess;
+  const int threads = 256;
+  const uint64_t work = aligned ? (n + 3) / 4 : n;
+  uint64_t blocks = (work + threads - 1) / threads;
+  const uint64_t cap = (uint64_t)sm_count * 8;  // 8 resident blocks per SM
+  if (blocks > cap) blocks = cap;
+  if (blocks == 0) blocks = 1;
+  // one compiled code path for every field selection: the 3-field and the
+  // 10-field calls give bit-identical values for the fields they share
+  (void)full;
+  if (aligned) fire_kernel<<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
+  else fire_kernel_scalar<<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+}  // namespace propag

@@ -1,0 +1,185 @@
+// Device-side arithmetic of the arrival-time propagation.
+//
+// Everything here is written with explicitly rounded operations
+// (__fadd_rn, __fmul_rn, __fmaf_rn, ...) so that the compiler can neither
+// contract nor reorder them: the result of every cell evaluation is a fixed
+// sequence of IEEE operations, the same one the CPU oracle performs.
+//
+// Semantics follow the reference kernel (paths relative to the reference
+// project):
+//   time_from                          crates/propag/src/propag.cu:269-294
+//   DDA line walk                      crates/propag/src/propag.h:91-135
+//   find_neighbor_which_reaches_first  crates/propag/src/propag.cu:124-190
+//   similar_fires / find_boundaries    crates/propag/src/propag.cu:296-302,345-375
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+namespace propag {
+
+constexpr uint32_t kNoRef = 0xFFFFFFFFu;  // refs_x = refs_y = 0xFFFF
+
+__device__ __forceinline__ uint32_t pack_ref(int x, int y) {
+  return (uint32_t)(x & 0xFFFF) | ((uint32_t)(y & 0xFFFF) << 16);
+}
+__device__ __forceinline__ int ref_x(uint32_t r) { return (int)(r & 0xFFFFu); }
+__device__ __forceinline__ int ref_y(uint32_t r) { return (int)(r >> 16); }
+
+// ---- portable float cosine / arctangent ------------------------------------
+// cos: Cody-Waite reduction by pi/2 with a three-part constant, Taylor
+// polynomials on [-pi/4, pi/4].  atan2: octant reduction; atan(t), t in [0,1],
+// with t > tan(pi/8) mapped through (t-1)/(t+1) and a Taylor series to u^19.
+// Both are accurate to about 1 ulp and, being plain IEEE operations, give the
+// same bits on every IEEE machine.
+__device__ __forceinline__ float pg_sin_poly(float r) {
+  const float r2 = __fmul_rn(r, r);
+  float p = __fmaf_rn(r2, 2.75573192e-6f, -1.98412698e-4f);
+  p = __fmaf_rn(r2, p, 8.33333333e-3f);
+  p = __fmaf_rn(r2, p, -1.66666667e-1f);
+  return __fmaf_rn(__fmul_rn(r, r2), p, r);
+}
+__device__ __forceinline__ float pg_cos_poly(float r) {
+  const float r2 = __fmul_rn(r, r);
+  float p = __fmaf_rn(r2, -2.75573192e-7f, 2.48015873e-5f);
+  p = __fmaf_rn(r2, p, -1.38888889e-3f);
+  p = __fmaf_rn(r2, p, 4.16666667e-2f);
+  p = __fmaf_rn(r2, p, -0.5f);
+  return __fmaf_rn(r2, p, 1.0f);
+}
+__device__ __forceinline__ float pg_cosf(float x) {
+  const float ax = fabsf(x);
+  const float k = rintf(__fmul_rn(ax, 0.636619772367581343f));
+  float r = __fmaf_rn(-k, 1.57079637050628662109375f, ax);
+  r = __fmaf_rn(-k, -4.37113900018624283e-8f, r);
+  r = __fmaf_rn(-k, -1.71512451677125e-15f, r);
+  switch (((int)k) & 3) {
+    case 0: return pg_cos_poly(r);
+    case 1: return -pg_sin_poly(r);
+    case 2: return -pg_cos_poly(r);
+    default: return pg_sin_poly(r);
+  }
+}
+__device__ __forceinline__ float pg_atan2f(float y, float x) {
+  const float ax = fabsf(x), ay = fabsf(y);
+  const float mx = ax > ay ? ax : ay;
+  const float mn = ax > ay ? ay : ax;
+  if (mx == 0.0f) return 0.0f;
+  const float t = __fdiv_rn(mn, mx);
+  float base = 0.0f;
+  float u = t;
+  if (t > 0.414213562373095049f) {
+    u = __fdiv_rn(__fsub_rn(t, 1.0f), __fadd_rn(t, 1.0f));
+    base = 0.785398163397448309616f;
+  }
+  const float u2 = __fmul_rn(u, u);
+  float p = __fmaf_rn(u2, 5.26315789e-2f, -5.88235294e-2f);
+  p = __fmaf_rn(u2, p, 6.66666667e-2f);
+  p = __fmaf_rn(u2, p, -7.69230769e-2f);
+  p = __fmaf_rn(u2, p, 9.09090909e-2f);
+  p = __fmaf_rn(u2, p, -1.11111111e-1f);
+  p = __fmaf_rn(u2, p, 1.42857143e-1f);
+  p = __fmaf_rn(u2, p, -2.00000000e-1f);
+  p = __fmaf_rn(u2, p, 3.33333333e-1f);
+  float a = __fadd_rn(__fmaf_rn(-__fmul_rn(u, u2), p, u), base);
+  if (ay > ax) a = __fsub_rn(1.57079632679489661923f, a);
+  if (x < 0.0f) a = __fsub_rn(3.14159265358979323846f, a);
+  if (y < 0.0f) a = -a;
+  return a;
+}
+
+// ---- time_from (propag.cu:269-294) -----------------------------------------
+// Arrival time at `to` for a fire that left `from` at `ftime`, spreading with
+// the elliptical speed of `fire` along the bearing from -> to.  The reference
+// writes `1.0 - ...` with double literals, so denom and factor are formed in
+// double and rounded to float; __frcp_rd / __fsqrt_rz as in the reference.
+struct Fire {
+  float speed_max, azimuth_max, eccentricity;
+};
+
+__device__ __forceinline__ float spread_factor(float azimuth, const Fire &f) {
+  const float angle = fabsf(__fsub_rn(azimuth, f.azimuth_max));
+  const float p = __fmul_rn(f.eccentricity, pg_cosf(angle));
+  const float denom = __double2float_rn(__dsub_rn(1.0, (double)p));
+  const double one_minus_e = __dsub_rn(1.0, (double)f.eccentricity);
+  return __double2float_rn(__dmul_rn(one_minus_e, (double)__frcp_rd(denom)));
+}
+
+__device__ __forceinline__ float step_time(float ftime, float distance, float speed) {
+  return __fadd_rn(ftime, __fmul_rn(distance, __frcp_rd(speed)));
+}
+
+__device__ __forceinline__ float cell_distance(int ddx, int ddy, float gdx, float gdy) {
+  const float dx = __fmul_rn((float)ddx, gdx);
+  const float dy = __fmul_rn((float)ddy, gdy);
+  return __fsqrt_rz(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+}
+
+__device__ __forceinline__ float bearing(int fx, int fy, int tx, int ty, bool north_up) {
+  return north_up ? pg_atan2f((float)(tx - fx), (float)(fy - ty))
+                  : pg_atan2f((float)(tx - fx), (float)(ty - fy));
+}
+
+__device__ __forceinline__ float time_from(int fx, int fy, float ftime, int tx, int ty,
+                                           const Fire &f, float gdx, float gdy, bool north_up) {
+  const float factor = spread_factor(bearing(fx, fy, tx, ty, north_up), f);
+  const float speed = __fmul_rn(f.speed_max, factor);
+  return step_time(ftime, cell_distance(fx - tx, fy - ty, gdx, gdy), speed);
+}
+
+// ---- DDA line-of-sight walk (propag.h:91-135) ------------------------------
+// Visits the cells from `from` to `to` inclusive in the reference's order and
+// reports whether one of them is a boundary.  The t-max accumulators are the
+// reference's float arithmetic: start 1/|d| (formed in double), step +1/|d|,
+// diagonal step when |tmax.x - tmax.y| < 1e-9.  The loop is bounded by
+// |dx| + |dy| + 2 visits, more than any walk takes.
+__device__ __forceinline__ bool is_boundary(const uint32_t *__restrict__ bnd, int64_t ix) {
+  return (__ldg(bnd + (ix >> 5)) >> (ix & 31)) & 1u;
+}
+
+__device__ __forceinline__ bool line_blocked(const uint32_t *__restrict__ bnd, int W, int fx,
+                                             int fy, int tx, int ty, uint32_t &steps) {
+  const int sx = (tx > fx) - (tx < fx), sy = (ty > fy) - (ty < fy);
+  const int adx = abs(tx - fx), ady = abs(ty - fy);
+  float tmx = __double2float_rn(1.0 / (double)(float)adx);
+  float tmy = __double2float_rn(1.0 / (double)(float)ady);
+  const float ddx = tmx, ddy = tmy;
+  int cx = fx, cy = fy;
+  const int limit = adx + ady + 2;
+  for (int n = 0; n < limit; ++n) {
+    const int px = cx, py = cy;
+    if (px == tx && py == ty) {
+      cx += sx;
+      cy += sy;
+    } else {
+      const bool vx = sx > 0 ? cx <= tx : cx >= tx;
+      const bool vy = sy > 0 ? cy <= ty : cy >= ty;
+      if (!(vx && vy)) return false;
+      if (fabsf(__fsub_rn(tmx, tmy)) < 1e-9f) {
+        cx += sx;
+        cy += sy;
+        tmx = __fadd_rn(tmx, ddx);
+        tmy = __fadd_rn(tmy, ddy);
+      } else if (tmx < tmy) {
+        cx += sx;
+        tmx = __fadd_rn(tmx, ddx);
+      } else {
+        cy += sy;
+        tmy = __fadd_rn(tmy, ddy);
+      }
+    }
+    ++steps;
+    if (is_boundary(bnd, (int64_t)px + (int64_t)py * W)) return true;
+  }
+  return false;
+}
+
+// similar_fires (propag.cu:296-302): float differences compared against the
+// reference's double thresholds.
+__device__ __forceinline__ bool similar_fires(const Fire &a, const Fire &b) {
+  return (double)fabsf(__fsub_rn(a.speed_max, b.speed_max)) < 0.1 &&
+         (double)fabsf(__fsub_rn(a.azimuth_max, b.azimuth_max)) < (5.0 * (2 * 3.14159265358979323846) / 360.0) &&
+         (double)fabsf(__fsub_rn(a.eccentricity, b.eccentricity)) < 0.05;
+}
+
+}  // namespace propag

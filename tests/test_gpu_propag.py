@@ -1,0 +1,162 @@
+"""Propagation kernels vs the CPU restatement of the reference kernel.
+
+Both sides run the reference's schedule (super-grid tiles of T cells, Jacobi
+sweeps inside a tile, tiles in row-major order, passes until no tile
+improves) on the same fire fields, with the same float arithmetic, so the
+comparison is exact: arrival times, references and boundary bits bit for bit,
+and the schedule counters (rounds, tile launches, sweeps, improvements)
+equal.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FMAX = np.finfo(np.float32).max
+
+
+def _fire(pp, terrain):
+    f = pp.fire_behaviour(terrain, full=False)
+    return f["speed_max"], f["azimuth_max"], f["eccentricity"]
+
+
+def _settings(pp, w, h, dx, dy, max_time):
+    gt = [0.0, dx, 0.0, 0.0 if dy > 0 else h * -dy, 0.0, dy]
+    g = pp.PyGeoReference(w, h, "+proj=utm +zone=30 +ellps=GRS80 +units=m +no_defs", gt)
+    return pp.PySettings(g, max_time)
+
+
+def _check(pp, oracle, terrain, w, h, dx, dy, max_time, ignitions, tile):
+    s = _settings(pp, w, h, dx, dy, max_time)
+    res = pp.propagate_arrays(s, terrain, ignitions, tile=tile)
+    sp, az, ec = _fire(pp, terrain)
+    o = oracle.propagate(w, h, dx, dy, max_time, sp, az, ec, ignitions,
+                         tile=(0 if tile == -1 else tile))
+    assert np.array_equal(res.boundary_change, o.boundaries), "boundary bits"
+    t_gpu = res.arrival_times.view(np.uint32)
+    t_ref = o.time.view(np.uint32)
+    diff = t_gpu != t_ref
+    if diff.any():
+        i = np.argwhere(diff)[0]
+        pytest.fail(f"{diff.sum()} times differ, first at {tuple(i)}: gpu={res.arrival_times[tuple(i)]} "
+                    f"ref={o.time[tuple(i)]}")
+    assert np.array_equal(res.refs_x.reshape(h, w), o.refs_x)
+    assert np.array_equal(res.refs_y.reshape(h, w), o.refs_y)
+    for k in ("rounds", "launches", "sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
+        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+    assert res.stats["burned"] == int(np.sum(o.time < FMAX))
+    return res, o
+
+
+def test_uniform_demo(pp, oracle):
+    w = h = 96
+    t = pp.demo_terrain(w, h)
+    _check(pp, oracle, t, w, h, 5.0, 5.0, 3000.0, [(40, 40, 0.0)], tile=-1)
+
+
+@pytest.mark.parametrize("tile", [-1, 57, 19])
+def test_hills_voronoi(pp, oracle, tile):
+    from py_propag import scenarios as S
+    sc = S.config0(size=128)
+    _check(pp, oracle, sc.terrain, sc.width, sc.height, sc.dx, sc.dy, sc.max_time,
+           sc.ignitions, tile)
+
+
+@pytest.mark.parametrize("tile", [-1, 64, 323])
+def test_ridges_lakes_roads_many_ignitions(pp, oracle, tile):
+    from py_propag import scenarios as S
+    sc = S.config1(size=160, n_ign=6, max_time=7200.0)
+    res, o = _check(pp, oracle, sc.terrain, sc.width, sc.height, sc.dx, sc.dy, sc.max_time,
+                    sc.ignitions, tile)
+    assert res.stats["improvements"] > 0
+
+
+def test_north_up_and_staggered_ignition_times(pp, oracle):
+    from py_propag import scenarios as S
+    sc = S.config0(size=96, seed=4)
+    ign = [(10, 10, 0.0), (80, 70, 600.0), (50, 20, 1200.0), (10, 10, 30.0)]  # repeated cell
+    _check(pp, oracle, sc.terrain, 96, 96, 5.0, -5.0, 20000.0, ign, tile=-1)
+
+
+def test_rectangular_and_degenerate_grids(pp, oracle):
+    for (w, h) in [(1, 1), (1, 37), (53, 1), (33, 70)]:
+        t = pp.demo_terrain(w, h)
+        _check(pp, oracle, t, w, h, 5.0, 5.0, 5000.0, [(0, 0, 0.0)], tile=-1)
+
+
+def test_no_ignition_and_non_burnable_ignition(pp, oracle):
+    w = h = 40
+    t = pp.demo_terrain(w, h)
+    res, _ = _check(pp, oracle, t, w, h, 5.0, 5.0, 5000.0, [], tile=-1)
+    assert res.stats["burned"] == 0
+    t["fuel_code"][20, 20] = 0
+    res, _ = _check(pp, oracle, t, w, h, 5.0, 5.0, 5000.0, [(20, 20, 0.0)], tile=-1)
+    assert res.stats["burned"] == 0  # a non-burnable ignition never spreads
+
+
+def _job(L, w, h, dx, dy, max_time, dev, tile=0):
+    j = L.PropagJob()
+    j.width, j.height, j.dx, j.dy, j.max_time, j.tile = w, h, dx, dy, max_time, tile
+    j.speed_max, j.azimuth_max, j.eccentricity = (dev[k].data_ptr() for k in ("sp", "az", "ec"))
+    j.ignitions, j.n_ignitions = dev["ign"].data_ptr(), dev["n_ign"]
+    j.time, j.refs_x, j.refs_y, j.boundaries = (dev[k].data_ptr() for k in ("time", "rx", "ry", "bnd"))
+    return j
+
+
+def _device_scenario(pp, sc):
+    import torch
+    sp, az, ec = _fire(pp, sc.terrain)
+    n = sc.width * sc.height
+    ign = np.array([(x, y, t) for (x, y, t) in sc.ignitions],
+                   dtype=[("x", "<u4"), ("y", "<u4"), ("t", "<f4")])
+    dev = dict(sp=torch.from_numpy(sp.ravel().copy()).cuda(), az=torch.from_numpy(az.ravel().copy()).cuda(),
+               ec=torch.from_numpy(ec.ravel().copy()).cuda(),
+               ign=torch.from_numpy(np.frombuffer(ign.tobytes() or bytes(12), np.uint8).copy()).cuda(),
+               n_ign=len(sc.ignitions),
+               time=torch.empty(n, dtype=torch.float32, device="cuda"),
+               rx=torch.empty(n, dtype=torch.int16, device="cuda"),
+               ry=torch.empty(n, dtype=torch.int16, device="cuda"),
+               bnd=torch.empty((n + 31) // 32, dtype=torch.int32, device="cuda"))
+    return dev
+
+
+@pytest.mark.parametrize("cluster", [1, 4, 16])
+def test_batch_equals_single_runs(pp, oracle, cluster):
+    """Uneven scenarios in one persistent launch give each scenario's own
+    result, whatever the cluster size."""
+    import torch
+    from py_propag import _lib as L
+    from py_propag import scenarios as S
+    scs = [S.config0(size=64, seed=11), S.config1(size=96, seed=12, n_ign=3, max_time=3600.0),
+           S.config0(size=80, seed=13), S.config1(size=48, seed=14, n_ign=2, max_time=1800.0)]
+    devs = [_device_scenario(pp, sc) for sc in scs]
+    jobs = [_job(L, sc.width, sc.height, sc.dx, sc.dy, sc.max_time, d,
+                 tile=(-1 if i % 2 == 0 else 37)) for i, (sc, d) in enumerate(zip(scs, devs))]
+    eng = pp.Engine(cluster=cluster)
+    stats = eng.run(jobs)
+    torch.cuda.synchronize()
+    for i, (sc, d, st) in enumerate(zip(scs, devs, stats)):
+        sp, az, ec = (d[k].cpu().numpy() for k in ("sp", "az", "ec"))
+        o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                             sc.ignitions, tile=(0 if i % 2 == 0 else 37))
+        assert np.array_equal(d["time"].cpu().numpy().view(np.uint32), o.time.ravel().view(np.uint32)), i
+        assert np.array_equal(d["rx"].cpu().numpy().view(np.uint16), o.refs_x.ravel()), i
+        assert st["sweeps"] == o.stats["sweeps"] and st["improvements"] == o.stats["improvements"], i
+    eng.close()
+
+
+def test_repeated_calls_are_deterministic(pp):
+    from py_propag import scenarios as S
+    sc = S.config0(size=100, seed=21)
+    s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
+    a = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=-1)
+    b = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=-1)
+    assert np.array_equal(a.arrival_times.view(np.uint32), b.arrival_times.view(np.uint32))
+    # schedule counters are deterministic; cycle counts and the number of
+    # referrer scans (which may or may not see a reference adopted in the
+    # same sweep) are not
+    keys = ("rounds", "launches", "sweeps", "evaluations", "improvements", "dda_steps", "gathers",
+            "burned")
+    assert {k: a.stats[k] for k in keys} == {k: b.stats[k] for k in keys}
