@@ -123,8 +123,9 @@ typedef struct PropagStats {
   uint64_t burned;       /* cells with time < FLT_MAX after the post mask */
   uint64_t gathers;      /* time[reference] reads (burning neighbours with a reference) */
   /* SM cycles the cluster leader spent per phase, barrier waits included:
-   * first sweeps of tile launches, evaluate, commit, referrer scans */
-  uint64_t cyc_first, cyc_eval, cyc_commit, cyc_scan;
+   * first sweeps of tile launches, evaluate, commit (with referrer scans),
+   * staging and write-back of shared-memory tiles */
+  uint64_t cyc_first, cyc_eval, cyc_commit, cyc_stage;
   uint32_t status;       /* 0 ok; nonzero: device-side error code */
   uint32_t max_walk;     /* longest line-of-sight walk (cells) */
 } PropagStats;

@@ -33,9 +33,9 @@ cudaError_t launch_prep(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells,
                         cudaStream_t stream);
 cudaError_t launch_ignite(const JobDev *jobs, uint32_t n_jobs, cudaStream_t stream);
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
-                          uint32_t n_slots, int csize, int threads, uint32_t *queue,
+                          uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
                           StatsDev *stats, unsigned long long max_sweeps, cudaStream_t stream);
-cudaError_t engine_max_clusters(int csize, int threads, int *n);
+cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n);
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
                         StatsDev *stats, cudaStream_t stream);
 
@@ -132,6 +132,9 @@ struct propag_engine {
   int csize = 0;    // 0 = auto
   int threads = 512;  // the engine kernel's launch bound
   int default_tile = PROPAG_DEFAULT_TILE;
+  size_t smem_budget = 200 * 1024;  // dynamic shared memory per CTA for resident tiles
+  int last_cluster = 0;             // cluster size and shared memory of the last run
+  size_t last_smem = 0;
   cudaStream_t stream = nullptr;  // the stream of the last run
   DevBuf job_scratch, slot_scratch, meta;
   JobDev *jobs_pinned = nullptr;
@@ -198,7 +201,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   // ---- validate and lay out per-job scratch ----
   std::vector<JobDev> jd(n_jobs);
   std::vector<size_t> off(n_jobs);
-  size_t job_bytes = 0, tn_max = 1;
+  std::vector<int> tw(n_jobs), th(n_jobs);
+  size_t job_bytes = 0;
   uint64_t max_cells = 1;
   for (uint32_t i = 0; i < n_jobs; ++i) {
     const PropagJob &j = jobs[i];
@@ -233,37 +237,64 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     d.out_rx = j.refs_x;
     d.out_ry = j.refs_y;
     d.out_bnd = j.boundaries;
+    tw[i] = std::min<int>(T, (int)j.width);
+    th[i] = std::min<int>(T, (int)j.height);
     off[i] = job_bytes;
-    job_bytes += align_up(N * 4, 256) * 3 + (j.boundaries ? 0 : align_up(words * 4, 256));
-    tn_max = std::max<size_t>(tn_max, (size_t)std::min<uint32_t>(T, j.width) * std::min<uint32_t>(T, j.height));
+    job_bytes += align_up(N * 4, 256) * 5 + (j.boundaries ? 0 : align_up(words * 4, 256));
     max_cells = std::max<uint64_t>(max_cells, N);
   }
   CK(e->job_scratch.reserve(job_bytes, stream));
   for (uint32_t i = 0; i < n_jobs; ++i) {
     const uint64_t N = (uint64_t)jd[i].W * jd[i].H;
     size_t o = off[i];
-    jd[i].refs = e->job_scratch.at<uint32_t>(o);
-    o += align_up(N * 4, 256);
-    jd[i].box_lo = e->job_scratch.at<uint32_t>(o);
-    o += align_up(N * 4, 256);
-    jd[i].box_hi = e->job_scratch.at<uint32_t>(o);
-    o += align_up(N * 4, 256);
+    uint32_t *arr[5];
+    for (int k = 0; k < 5; ++k) {
+      arr[k] = e->job_scratch.at<uint32_t>(o);
+      o += align_up(N * 4, 256);
+    }
+    jd[i].refs = arr[0];
+    jd[i].box_x0 = arr[1];
+    jd[i].box_y0 = arr[2];
+    jd[i].box_x1 = arr[3];
+    jd[i].box_y1 = arr[4];
     jd[i].bnd = jobs[i].boundaries ? jobs[i].boundaries : e->job_scratch.at<uint32_t>(o);
   }
-  // ---- cluster slots ----
+  // ---- cluster size and tile residency ----
+  // A tile launch runs in the cluster's shared memory when the tile and its
+  // halo fit in the dynamic shared-memory budget of the cluster's CTAs.
+  const size_t budget = e->smem_budget;
+  auto fits = [&](uint32_t i, int c) { return smem_bytes(tw[i], th[i], c) <= budget; };
   int csize = e->csize;
-  int max_clusters = 0;
   if (csize == 0) {
-    // enough clusters for every job, as large as the machine allows
-    int per_sm = 0;
-    CK(engine_max_clusters(1, e->threads, &per_sm));  // = resident CTAs
-    const int ctas = std::max(per_sm, 1);
-    csize = 1;
-    while (csize < 16 && (uint64_t)(csize * 2) * n_jobs <= (uint64_t)ctas) csize *= 2;
+    // the smallest cluster that holds every job's tile (more clusters, more
+    // scenarios at once); when some tile never fits, as many clusters as
+    // there are jobs, as large as the machine allows
+    for (int c = 1; c <= 16 && csize == 0; c *= 2) {
+      bool all = true;
+      for (uint32_t i = 0; i < n_jobs && all; ++i) all = fits(i, c);
+      if (all) csize = c;
+    }
+    if (csize == 0) {
+      int ctas = 0;
+      CK(engine_max_clusters(1, e->threads, 0, &ctas));
+      csize = 1;
+      while (csize < 16 && (uint64_t)(csize * 2) * n_jobs <= (uint64_t)std::max(ctas, 1)) csize *= 2;
+    }
   }
-  CK(engine_max_clusters(csize, e->threads, &max_clusters));
+  size_t smem = 0, tn_max = 1;
+  for (uint32_t i = 0; i < n_jobs; ++i) {
+    jd[i].smem_tile = fits(i, csize) ? 1 : 0;
+    if (jd[i].smem_tile)
+      smem = std::max(smem, smem_bytes(tw[i], th[i], csize));
+    else
+      tn_max = std::max<size_t>(tn_max, (size_t)tw[i] * (size_t)th[i]);
+  }
+  int max_clusters = 0;
+  CK(engine_max_clusters(csize, e->threads, smem, &max_clusters));
   if (max_clusters < 1) return fail(PROPAG_ERR_CUDA, "cluster size " + std::to_string(csize) + " cannot be resident");
   const uint32_t n_slots = std::min<uint32_t>(n_jobs, (uint32_t)max_clusters);
+  e->last_cluster = csize;
+  e->last_smem = smem;
   const size_t words_max = tn_max / 32 + 1;
   const size_t slot_bytes = align_up(tn_max * 4, 256) * 3 + align_up(words_max * 4, 256) +
                             align_up(tn_max * sizeof(Update), 256) + 256;
@@ -318,7 +349,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   CK(launch_prep(d_jobs, n_jobs, max_cells, e->sms, stream));
   CK(launch_ignite(d_jobs, n_jobs, stream));
   CK(cudaEventRecord(e->ev[1], stream));
-  CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, d_queue, d_stats,
+  CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, smem, d_queue, d_stats,
                    1ull << 40, stream));
   CK(cudaEventRecord(e->ev[2], stream));
   CK(launch_post(d_jobs, n_jobs, max_cells, e->sms, d_stats, stream));
@@ -342,7 +373,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
       o.cyc_first = hs[i].cyc_first;
       o.cyc_eval = hs[i].cyc_eval;
       o.cyc_commit = hs[i].cyc_commit;
-      o.cyc_scan = hs[i].cyc_scan;
+      o.cyc_stage = hs[i].cyc_stage;
       o.status = hs[i].status;
       o.max_walk = hs[i].max_walk;
     }

@@ -24,10 +24,18 @@
 //
 // Mapping.  One thread-block cluster works on one scenario at a time and
 // pulls scenarios from a queue, so a batch of scenarios runs concurrently,
-// each on its own cluster, in one launch.  A sweep has three phases
-// separated by cluster barriers: evaluate (reads only), commit (writes state,
-// marks the next sweep's cells), referrer scans (marks more cells).
-// Cluster barriers are hardware barriers: there is no spin-wait anywhere.
+// each on its own cluster, in one launch.  A sweep is two phases separated by
+// cluster barriers: evaluate (reads only) and commit (writes the state, marks
+// the next sweep's cells, scans referrer boxes).  Cluster barriers are
+// hardware barriers: there is no spin-wait anywhere.
+//
+// A tile launch runs in one of two modes:
+//   * shared-memory tile: the tile and its halo (time, reference, referrer
+//     boxes) are staged into the distributed shared memory of the cluster,
+//     rows dealt round-robin to the CTAs; all sweeps read and write there and
+//     the tile is written back at the end of the launch;
+//   * global tile (tiles too large for the cluster's shared memory): the state
+//     stays in global memory and the work lists in the slot's scratch.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -40,6 +48,10 @@
 namespace cg = cooperative_groups;
 
 namespace propag {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kEngineThreads = 512;
+constexpr uint32_t kEmptyBox = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------- prep ----
 // Boundary bits (find_boundaries) packed with a warp ballot, plus the initial
@@ -70,10 +82,12 @@ __global__ void __launch_bounds__(256) prep_kernel(const JobDev *__restrict__ jo
       }
       j.time[i] = FLT_MAX;
       j.refs[i] = kNoRef;
-      j.box_lo[i] = 0xFFFFFFFFu;
-      j.box_hi[i] = 0u;
+      j.box_x0[i] = kEmptyBox;
+      j.box_y0[i] = kEmptyBox;
+      j.box_x1[i] = 0u;
+      j.box_y1[i] = 0u;
     }
-    const unsigned word = __ballot_sync(0xFFFFFFFFu, b);
+    const unsigned word = __ballot_sync(kFull, b);
     if (lane == 0) j.bnd[w0 >> 5] = word;
   }
 }
@@ -98,21 +112,18 @@ __global__ void ignite_kernel(const JobDev *__restrict__ jobs) {
     if (ign[k].x >= (uint32_t)j.W || ign[k].y >= (uint32_t)j.H) continue;
     const int64_t c = ign[k].x + (int64_t)ign[k].y * j.W;
     if (j.time[c] != FLT_MAX) {
-      const uint32_t r = pack_ref(ign[k].x, ign[k].y);
-      j.refs[c] = r;
-      j.box_lo[c] = r;
-      j.box_hi[c] = r;
+      j.refs[c] = pack_ref(ign[k].x, ign[k].y);
+      j.box_x0[c] = j.box_x1[c] = ign[k].x;
+      j.box_y0[c] = j.box_y1[c] = ign[k].y;
     }
   }
 }
 
-// -------------------------------------------------------------- engine ----
+// ------------------------------------------------------- common pieces ----
 struct Best {
   float time;
   uint32_t ref;
 };
-
-constexpr unsigned kFull = 0xFFFFFFFFu;
 
 __device__ __noinline__ bool line_blocked_call(const uint32_t *__restrict__ bnd, int W, int fx,
                                                int fy, int tx, int ty, uint32_t &steps) {
@@ -139,48 +150,22 @@ __device__ __forceinline__ void dir_consts(const JobDev &j, DirConst &d) {
   }
 }
 
-// find_neighbor_which_reaches_first (propag.cu:124-190) on the current state.
-// All loads are issued in three independent waves (neighbour times and
-// speeds; references; reference times and the rest of the neighbours'
-// fire) before the reference's sequential decision logic runs over the
-// neighbours in its order, in registers.
-__device__ __forceinline__ Best evaluate(const JobDev &j, const DirConst &dc, int x, int y,
-                                         uint32_t &dda, uint32_t &gat, uint32_t &walk_max) {
-  const int W = j.W, H = j.H;
-  const int64_t me = x + (int64_t)y * W;
-  Best best{__ldcg(j.time + me), __ldcg(j.refs + me)};
+struct Counters {
+  uint32_t dda = 0, gat = 0, walk_max = 0;
+  unsigned long long evals = 0, scans = 0;
+};
+
+// find_neighbor_which_reaches_first (propag.cu:124-190) given the already
+// fetched state of the eight neighbours: nt (times), fs/fa/fe (fire), nr
+// (references), rt (times of the references), act (bit k: neighbour k is
+// burning, in the grid and not referencing the cell).  Runs the reference's
+// sequential decision logic over the neighbours in its order, in registers.
+__device__ __forceinline__ Best decide(const JobDev &j, const DirConst &dc, int x, int y,
+                                       Best best, const float nt[8], const float fs[8],
+                                       const float fa[8], const float fe[8], const uint32_t nr[8],
+                                       const float rt[8], uint32_t act, Counters &cnt) {
   const bool nu = j.north_up != 0;
-  float nt[8], rt[8], fs[8], fa[8], fe[8];
-  uint32_t nr[8];
-  uint32_t act = 0;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int kk = k < 4 ? k : k + 1;
-    const int nx = x + kk % 3 - 1, ny = y + kk / 3 - 1;
-    const bool inb = nx >= 0 && ny >= 0 && nx < W && ny < H;
-    const int64_t n = nx + (int64_t)ny * W;
-    nt[k] = inb ? __ldcg(j.time + n) : FLT_MAX;
-    fs[k] = inb ? __ldg(j.speed + n) : 0.0f;
-  }
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    if (nt[k] < j.max_time && fs[k] != 0.0f) act |= 1u << k;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int kk = k < 4 ? k : k + 1;
-    const int64_t n = (x + kk % 3 - 1) + (int64_t)(y + kk / 3 - 1) * W;
-    const bool a = (act >> k) & 1u;
-    nr[k] = a ? __ldcg(j.refs + n) : kNoRef;
-    fa[k] = a ? __ldg(j.az + n) : 0.0f;
-    fe[k] = a ? __ldg(j.ecc + n) : 0.0f;
-  }
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    if (ref_x(nr[k]) == x && ref_y(nr[k]) == y) act &= ~(1u << k);  // its reference is me
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    rt[k] = (act >> k) & 1u ? __ldcg(j.time + ref_x(nr[k]) + (int64_t)ref_y(nr[k]) * W) : FLT_MAX;
-  gat += __popc(act);
+  cnt.gat += __popc(act);
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     if (!((act >> k) & 1u)) continue;
@@ -192,9 +177,9 @@ __device__ __forceinline__ Best evaluate(const JobDev &j, const DirConst &dc, in
     float cand = time_from(rx, ry, rt[k], x, y, f, j.gdx, j.gdy, nu);
     if (cand < ntime && cand < best.time) {
       uint32_t cref = nr[k];
-      const uint32_t before = dda;
-      const bool blocked = line_blocked_call(j.bnd, W, nx, ny, rx, ry, dda);
-      walk_max = max(walk_max, dda - before);
+      const uint32_t before = cnt.dda;
+      const bool blocked = line_blocked_call(j.bnd, j.W, nx, ny, rx, ry, cnt.dda);
+      cnt.walk_max = max(cnt.walk_max, cnt.dda - before);
       if (blocked) {
         cref = pack_ref(nx, ny);
         cand = ntime;
@@ -227,11 +212,141 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *counter, uint32_t cnt,
   return base + x - cnt;
 }
 
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, uint32_t lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, v, o);
+    if (lane >= (uint32_t)o) v += y;
+  }
+  return v;
+}
+
+// Referrer box of a changed cell clipped to the tile grown by one cell
+// (referrers further out have no neighbour inside the tile).
+struct Box {
+  int x0, y0, x1, y1;
+  __device__ __forceinline__ uint32_t area() const {
+    return x0 > x1 || y0 > y1 ? 0u : (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+  }
+};
+
+__device__ __forceinline__ Box clip_box(int bx0, int by0, int bx1, int by1, int tx0, int ty0,
+                                        int TW, int TH, int W, int H) {
+  Box b;
+  b.x0 = max(max(bx0, tx0 - 1), 0);
+  b.y0 = max(max(by0, ty0 - 1), 0);
+  b.x1 = min(min(bx1, tx0 + TW), W - 1);
+  b.y1 = min(min(by1, ty0 + TH), H - 1);
+  return b;
+}
+
+// One lane's referrer box in a warp's concatenated scan.
+struct ScanBox {
+  int x0, y0;
+  uint32_t bw, want, incl;  // width, packed reference, inclusive end in the concatenation
+};
+
+// Walks the concatenation of the warp's boxes, 32 cells per step, so that a
+// step is one independent wave of loads; mark_fn(hit, gx, gy) is called once
+// per step by every lane.  ref_fn(gx, gy, t) returns a cell's reference and
+// time.
+template <typename RefFn, typename MarkFn>
+__device__ __forceinline__ void warp_scan_boxes(ScanBox *sb, const Box &box, uint32_t want,
+                                                uint32_t lane, Counters &cnt, RefFn ref_fn,
+                                                MarkFn mark_fn) {
+  const uint32_t area = box.area();
+  cnt.scans += area ? 1 : 0;
+  const uint32_t incl = warp_incl_scan(area, lane);
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  sb[lane] = ScanBox{box.x0, box.y0, (uint32_t)max(box.x1 - box.x0 + 1, 1), want, incl};
+  __syncwarp();
+  for (uint32_t q0 = 0; q0 < total; q0 += 32) {
+    const uint32_t q = q0 + lane;
+    bool hit = false;
+    int xx = 0, yy = 0;
+    if (q < total) {
+      int lo = 0, hi = 31;  // first lane whose inclusive end exceeds q
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (sb[mid].incl > q) hi = mid; else lo = mid + 1;
+      }
+      const ScanBox o = sb[lo];
+      const uint32_t a = q - (lo ? sb[lo - 1].incl : 0u);  // offset in lane lo's box
+      xx = o.x0 + (int)(a % o.bw);
+      yy = o.y0 + (int)(a / o.bw);
+      float t;
+      const uint32_t r = ref_fn(xx, yy, t);
+      hit = r == o.want && t < FLT_MAX;
+    }
+    mark_fn(hit, xx, yy);
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void sync_cluster() {
+  __threadfence();
+  cg::this_cluster().sync();
+}
+
+// Referrer box update for a cell (x, y) that adopted reference r, in the
+// global arrays (fire-and-forget reductions).
+__device__ __forceinline__ void box_expand_global(const JobDev &j, uint32_t r, int x, int y) {
+  const int64_t rc = ref_x(r) + (int64_t)ref_y(r) * j.W;
+  atomicMin(j.box_x0 + rc, (uint32_t)x);
+  atomicMin(j.box_y0 + rc, (uint32_t)y);
+  atomicMax(j.box_x1 + rc, (uint32_t)x);
+  atomicMax(j.box_y1 + rc, (uint32_t)y);
+}
+
+struct TileDesc {
+  int x0, y0, TW, TH;
+};
+
+// ================================================ global-memory tiles ====
+__device__ __forceinline__ Best evaluate_global(const JobDev &j, const DirConst &dc, int x, int y,
+                                                Counters &cnt) {
+  const int W = j.W, H = j.H;
+  const int64_t me = x + (int64_t)y * W;
+  Best best{__ldcg(j.time + me), __ldcg(j.refs + me)};
+  float nt[8], rt[8], fs[8], fa[8], fe[8];
+  uint32_t nr[8];
+  uint32_t act = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int kk = k < 4 ? k : k + 1;
+    const int nx = x + kk % 3 - 1, ny = y + kk / 3 - 1;
+    const bool inb = nx >= 0 && ny >= 0 && nx < W && ny < H;
+    const int64_t n = nx + (int64_t)ny * W;
+    nt[k] = inb ? __ldcg(j.time + n) : FLT_MAX;
+    fs[k] = inb ? __ldg(j.speed + n) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (nt[k] < j.max_time && fs[k] != 0.0f) act |= 1u << k;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int kk = k < 4 ? k : k + 1;
+    const int64_t n = (x + kk % 3 - 1) + (int64_t)(y + kk / 3 - 1) * W;
+    const bool a = (act >> k) & 1u;
+    nr[k] = a ? __ldcg(j.refs + n) : kNoRef;
+    fa[k] = a ? __ldg(j.az + n) : 0.0f;
+    fe[k] = a ? __ldg(j.ecc + n) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (ref_x(nr[k]) == x && ref_y(nr[k]) == y) act &= ~(1u << k);  // its reference is me
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    rt[k] = (act >> k) & 1u ? __ldcg(j.time + ref_x(nr[k]) + (int64_t)ref_y(nr[k]) * W) : FLT_MAX;
+  return decide(j, dc, x, y, best, nt, fs, fa, fe, nr, rt, act, cnt);
+}
+
 // Marks the 3x3 neighbourhood of tile cell (lx, ly) for the next sweep
 // (deduplicated through the dirty bitmap) and appends the new cells to work
 // list q.  Called by every lane of a warp; `active` selects the lanes.
-__device__ __forceinline__ void mark3x3(const SlotDev &s, int q, bool active, int lx, int ly,
-                                        int TW, int TH, uint32_t lane) {
+__device__ __forceinline__ void mark3x3_list(const SlotDev &s, int q, bool active, int lx, int ly,
+                                             int TW, int TH, uint32_t lane) {
   uint32_t fresh = 0;
   if (active) {
 #pragma unroll
@@ -253,74 +368,450 @@ __device__ __forceinline__ void mark3x3(const SlotDev &s, int q, bool active, in
   }
 }
 
-__device__ __forceinline__ void box_min(uint32_t *w, int x, int y) {
-  uint32_t old = __ldcg(w);
-  for (;;) {
-    const uint32_t ox = old & 0xFFFFu, oy = old >> 16;
-    const uint32_t nw = min(ox, (uint32_t)x) | (min(oy, (uint32_t)y) << 16);
-    if (nw == old) return;
-    const uint32_t prev = atomicCAS(w, old, nw);
-    if (prev == old) return;
-    old = prev;
-  }
-}
-__device__ __forceinline__ void box_max(uint32_t *w, int x, int y) {
-  uint32_t old = __ldcg(w);
-  for (;;) {
-    const uint32_t ox = old & 0xFFFFu, oy = old >> 16;
-    const uint32_t nw = max(ox, (uint32_t)x) | (max(oy, (uint32_t)y) << 16);
-    if (nw == old) return;
-    const uint32_t prev = atomicCAS(w, old, nw);
-    if (prev == old) return;
-    old = prev;
-  }
-}
-
-__device__ __forceinline__ void sync_cluster() {
-  __threadfence();
-  cg::this_cluster().sync();
-}
-
-// Referrer box of a changed cell, clipped to the tile grown by one cell
-// (referrers further out have no neighbour inside the tile).
-struct Box {
-  int x0, y0, x1, y1;
-  __device__ __forceinline__ uint32_t area() const {
-    return x0 > x1 || y0 > y1 ? 0u : (uint32_t)(x1 - x0 + 1) * (uint32_t)(y1 - y0 + 1);
+struct SweepCtx {
+  bool leader;
+  Counters cnt;
+  unsigned long long sweeps = 0, improvements = 0, max_sweeps = 0;
+  unsigned long long cyc[4] = {0, 0, 0, 0};  // first sweeps, evaluate, commit, staging
+  long long t_phase = 0;
+  bool abort = false;
+  __device__ __forceinline__ void tick(int phase) {
+    if (leader) {
+      const long long now = clock64();
+      cyc[phase] += (unsigned long long)(now - t_phase);
+      t_phase = now;
+    }
   }
 };
 
-__device__ __forceinline__ Box clipped_box(const JobDev &j, uint32_t c, int tx0, int ty0, int TW,
-                                           int TH) {
-  const uint32_t lo = __ldcg(j.box_lo + c), hi = __ldcg(j.box_hi + c);
-  Box b;
-  b.x0 = max(max((int)(lo & 0xFFFFu), tx0 - 1), 0);
-  b.y0 = max(max((int)(lo >> 16), ty0 - 1), 0);
-  b.x1 = min(min((int)(hi & 0xFFFFu), tx0 + TW), j.W - 1);
-  b.y1 = min(min((int)(hi >> 16), ty0 + TH), j.H - 1);
-  return b;
+// One tile launch with the state in global memory.  Returns whether any
+// sweep improved a cell.
+__device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &s, const TileDesc &td,
+                            ScanBox *scan_boxes, uint32_t tid, uint32_t nthreads, SweepCtx &cx) {
+  const uint32_t lane = threadIdx.x & 31, gwarp = tid >> 5;
+  const int x0 = td.x0, y0 = td.y0, TW = td.TW, TH = td.TH;
+  const uint32_t TN = (uint32_t)TW * (uint32_t)TH;
+  bool first = true, worked = false;
+  int p = 0;
+  for (;;) {
+    // ---- evaluate (Jacobi: nothing is written to the state) ----
+    const uint32_t nitems = first ? TN : __ldcg(s.ctr + p);
+    ++cx.sweeps;  // every thread counts, so the abort below is uniform
+    if (cx.leader) {
+      s.ctr[p ^ 1] = 0;
+      cx.cnt.evals += nitems;
+    }
+    for (uint32_t base = gwarp * 32; base < nitems; base += nthreads) {
+      const uint32_t i = base + lane;
+      bool improved = false;
+      Best b{0.0f, 0u};
+      uint32_t k = i;
+      if (i < nitems) {
+        if (!first) {
+          k = __ldcg(s.cand[p] + i);
+          atomicAnd(s.dirty + (k >> 5), ~(1u << (k & 31)));
+        }
+        const int x = x0 + (int)(k % (uint32_t)TW), y = y0 + (int)(k / (uint32_t)TW);
+        b = evaluate_global(j, dc, x, y, cx.cnt);
+        improved = b.time < __ldcg(j.time + x + (int64_t)y * j.W);
+      }
+      const uint32_t at = warp_append(s.ctr + 2, improved ? 1u : 0u, lane);
+      if (improved) s.upd[at] = Update{k, b.time, b.ref, 0u};
+    }
+    sync_cluster();
+    cx.tick(first ? 0 : 1);
+    const uint32_t nupd = __ldcg(s.ctr + 2);
+    if (nupd == 0) break;
+    worked = true;
+    // ---- commit (update_point / commit_point), mark, referrer scans ----
+    // A referrer scan may run while other cells of this sweep commit: a cell
+    // whose reference changes in this sweep is itself marked, and a box only
+    // grows, so what the scan must find (referrers from earlier sweeps) is
+    // unaffected by the concurrent writes.
+    for (uint32_t base = gwarp * 32; base < nupd; base += nthreads) {
+      const uint32_t u = base + lane;
+      const bool valid = u < nupd;
+      int lx = 0, ly = 0;
+      uint32_t want = 0;
+      Box box{1, 1, 0, 0};
+      if (valid) {
+        const Update up = s.upd[u];
+        lx = (int)(up.k % (uint32_t)TW);
+        ly = (int)(up.k / (uint32_t)TW);
+        const int x = x0 + lx, y = y0 + ly;
+        const int64_t c = x + (int64_t)y * j.W;
+        j.time[c] = up.time;
+        j.refs[c] = up.ref;
+        box_expand_global(j, up.ref, x, y);
+        want = pack_ref(x, y);
+        const uint32_t bx0 = __ldcg(j.box_x0 + c);
+        if (bx0 != kEmptyBox)
+          box = clip_box((int)bx0, (int)__ldcg(j.box_y0 + c), (int)__ldcg(j.box_x1 + c),
+                         (int)__ldcg(j.box_y1 + c), x0, y0, TW, TH, j.W, j.H);
+      }
+      mark3x3_list(s, p ^ 1, valid, lx, ly, TW, TH, lane);
+      warp_scan_boxes(
+          scan_boxes + (threadIdx.x & ~31u), box, want, lane, cx.cnt,
+          [&](int xx, int yy, float &t) {
+            const int64_t n = xx + (int64_t)yy * j.W;
+            t = __ldcg(j.time + n);
+            return __ldcg(j.refs + n);
+          },
+          [&](bool hit, int xx, int yy) {
+            if (__any_sync(kFull, hit)) mark3x3_list(s, p ^ 1, hit, xx - x0, yy - y0, TW, TH, lane);
+          });
+    }
+    sync_cluster();
+    cx.tick(2);
+    if (cx.leader) {
+      cx.improvements += nupd;
+      s.ctr[2] = 0;  // the update list was consumed
+    }
+    p ^= 1;
+    first = false;
+    if (cx.sweeps > cx.max_sweeps) {
+      cx.abort = true;
+      break;
+    }
+  }
+  return worked;
 }
 
-// One cell of a referrer scan: does (xx, yy) reference `want`?
-__device__ __forceinline__ bool refers(const JobDev &j, int xx, int yy, uint32_t want) {
-  const int64_t n = xx + (int64_t)yy * j.W;
-  return __ldcg(j.refs + n) == want && __ldcg(j.time + n) < FLT_MAX;
-}
-
-// One lane's referrer box in the warp's concatenated scan.
-struct ScanBox {
-  int x0, y0;
-  uint32_t bw, want, incl;  // width, packed reference, inclusive end in the concatenation
+// ================================================ shared-memory tiles ====
+// Cell slots of the tile and its halo: halo coordinates hx in [0, TW + 2),
+// hy in [0, TH + 2) (grid x = x0 - 1 + hx, y = y0 - 1 + hy); row hy lives in
+// CTA hy % C at local row hy / C.
+struct SmemTile {
+  float *time;
+  uint32_t *ref;
+  uint32_t *blo, *bhi;  // referrer box corners, x | y << 16 (blo 0xFFFFFFFF = empty)
+  float *utime;         // pending updates: time, reference, local slot
+  uint32_t *uref;
+  uint16_t *list;       // this sweep's cells to evaluate (local slot index)
+  uint16_t *uidx;
+  uint32_t *dirty;      // bit per local slot: evaluate in the next sweep
+  uint32_t *ctr;        // [0] list size, [1] local updates, [2..3] cluster updates (parity)
 };
 
-constexpr int kEngineThreads = 512;
+__device__ __forceinline__ SmemTile carve_smem(char *base, int cap) {
+  SmemTile t;
+  t.time = (float *)base;
+  base += (size_t)cap * 4;
+  t.ref = (uint32_t *)base;
+  base += (size_t)cap * 4;
+  t.blo = (uint32_t *)base;
+  base += (size_t)cap * 4;
+  t.bhi = (uint32_t *)base;
+  base += (size_t)cap * 4;
+  t.utime = (float *)base;
+  base += (size_t)cap * 4;
+  t.uref = (uint32_t *)base;
+  base += (size_t)cap * 4;
+  t.list = (uint16_t *)base;
+  base += (size_t)cap * 2;
+  t.uidx = (uint16_t *)base;
+  base += (size_t)cap * 2;
+  t.dirty = (uint32_t *)(((uintptr_t)base + 3) & ~(uintptr_t)3);
+  base = (char *)(t.dirty + (cap / 32 + 1));
+  t.ctr = (uint32_t *)(((uintptr_t)base + 15) & ~(uintptr_t)15);
+  return t;
+}
 
+struct SmemGeom {
+  int x0, y0, TW, TH, P, HR, C, rank, rows_mine;
+};
+
+template <typename T>
+__device__ __forceinline__ T *rank_ptr(T *local, int r) {
+  return cg::this_cluster().map_shared_rank(local, (unsigned)r);
+}
+
+__device__ __forceinline__ uint32_t box_pack_min(uint32_t old, int x, int y) {
+  return min(old & 0xFFFFu, (uint32_t)x) | (min(old >> 16, (uint32_t)y) << 16);
+}
+__device__ __forceinline__ uint32_t box_pack_max(uint32_t old, int x, int y) {
+  return max(old & 0xFFFFu, (uint32_t)x) | (max(old >> 16, (uint32_t)y) << 16);
+}
+
+// Marks the tile cells of the 3x3 neighbourhood of halo cell (hx, hy) in
+// their owners' dirty bitmaps (fire-and-forget reductions on shared memory).
+__device__ __forceinline__ void mark3x3_smem(const SmemTile &sm, const SmemGeom &g, int hx, int hy) {
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    const int ax = hx + t % 3 - 1, ay = hy + t / 3 - 1;
+    if (ax < 1 || ay < 1 || ax > g.TW || ay > g.TH) continue;
+    const int owner = ay % g.C;
+    const uint32_t li = (uint32_t)((ay / g.C) * g.P + ax);
+    uint32_t *d = owner == g.rank ? sm.dirty : rank_ptr(sm.dirty, owner);
+    atomicOr(d + (li >> 5), 1u << (li & 31));
+  }
+}
+
+__device__ __forceinline__ void smem_cell(const SmemTile &sm, const SmemGeom &g, int hx, int hy,
+                                          float &t, uint32_t &r) {
+  const int owner = hy % g.C;
+  const int li = (hy / g.C) * g.P + hx;
+  if (owner == g.rank) {
+    t = sm.time[li];
+    r = sm.ref[li];
+  } else {
+    t = rank_ptr(sm.time, owner)[li];
+    r = rank_ptr(sm.ref, owner)[li];
+  }
+}
+
+__device__ __forceinline__ float smem_time_of(const JobDev &j, const SmemTile &sm,
+                                              const SmemGeom &g, uint32_t r) {
+  const int hx = ref_x(r) - (g.x0 - 1), hy = ref_y(r) - (g.y0 - 1);
+  if (hx >= 0 && hy >= 0 && hx < g.P && hy < g.HR) {
+    const int owner = hy % g.C;
+    const int li = (hy / g.C) * g.P + hx;
+    return owner == g.rank ? sm.time[li] : rank_ptr(sm.time, owner)[li];
+  }
+  return __ldcg(j.time + ref_x(r) + (int64_t)ref_y(r) * j.W);  // outside: static this launch
+}
+
+__device__ __forceinline__ Best evaluate_smem(const JobDev &j, const DirConst &dc,
+                                              const SmemTile &sm, const SmemGeom &g, int hx,
+                                              int hy, Counters &cnt) {
+  const int x = g.x0 - 1 + hx, y = g.y0 - 1 + hy;
+  Best best;
+  smem_cell(sm, g, hx, hy, best.time, best.ref);
+  float nt[8], rt[8], fs[8], fa[8], fe[8];
+  uint32_t nr[8];
+  uint32_t act = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int kk = k < 4 ? k : k + 1;
+    const int di = kk % 3 - 1, dj = kk / 3 - 1;
+    const int nx = x + di, ny = y + dj;
+    const bool inb = nx >= 0 && ny >= 0 && nx < j.W && ny < j.H;
+    smem_cell(sm, g, hx + di, hy + dj, nt[k], nr[k]);  // outside the grid: FLT_MAX, no reference
+    fs[k] = inb ? __ldg(j.speed + nx + (int64_t)ny * j.W) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (nt[k] < j.max_time && fs[k] != 0.0f && !(ref_x(nr[k]) == x && ref_y(nr[k]) == y))
+      act |= 1u << k;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int kk = k < 4 ? k : k + 1;
+    const int64_t n = (x + kk % 3 - 1) + (int64_t)(y + kk / 3 - 1) * j.W;
+    const bool a = (act >> k) & 1u;
+    fa[k] = a ? __ldg(j.az + n) : 0.0f;
+    fe[k] = a ? __ldg(j.ecc + n) : 0.0f;
+    rt[k] = a ? smem_time_of(j, sm, g, nr[k]) : FLT_MAX;
+  }
+  return decide(j, dc, x, y, best, nt, fs, fa, fe, nr, rt, act, cnt);
+}
+
+__device__ __forceinline__ void smem_box_cas(uint32_t *w, int x, int y, bool is_min) {
+  uint32_t o = *w;
+  for (;;) {
+    const uint32_t nw = is_min ? box_pack_min(o, x, y) : box_pack_max(o, x, y);
+    if (nw == o) return;
+    const uint32_t pr = atomicCAS(w, o, nw);
+    if (pr == o) return;
+    o = pr;
+  }
+}
+
+// One tile launch resident in the cluster's shared memory.
+__device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const TileDesc &td,
+                          ScanBox *scan_boxes, SweepCtx &cx) {
+  cg::cluster_group cluster = cg::this_cluster();
+  SmemGeom g;
+  g.x0 = td.x0;
+  g.y0 = td.y0;
+  g.TW = td.TW;
+  g.TH = td.TH;
+  g.P = td.TW + 2;
+  g.HR = td.TH + 2;
+  g.C = (int)cluster.num_blocks();
+  g.rank = (int)cluster.block_rank();
+  g.rows_mine = g.HR > g.rank ? (g.HR - g.rank + g.C - 1) / g.C : 0;
+  const SmemTile sm = carve_smem(smem, smem_cap(td.TW, td.TH, g.C));
+  const uint32_t lane = threadIdx.x & 31;
+  const int nslots = g.rows_mine * g.P;
+  const int nwords = (nslots + 31) / 32;
+
+  // ---- stage the tile and its halo (state, referrer boxes) ----
+  for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
+    const int lr = s / g.P, hx = s % g.P;
+    const int hy = g.rank + lr * g.C;
+    const int gx = g.x0 - 1 + hx, gy = g.y0 - 1 + hy;
+    float t = FLT_MAX;
+    uint32_t r = kNoRef, lo = kEmptyBox, hi = 0;
+    if (gx >= 0 && gy >= 0 && gx < j.W && gy < j.H) {
+      const int64_t c = gx + (int64_t)gy * j.W;
+      t = __ldcg(j.time + c);
+      r = __ldcg(j.refs + c);
+      const uint32_t bx0 = __ldcg(j.box_x0 + c);
+      if (bx0 != kEmptyBox) {
+        lo = bx0 | (__ldcg(j.box_y0 + c) << 16);
+        hi = __ldcg(j.box_x1 + c) | (__ldcg(j.box_y1 + c) << 16);
+      }
+    }
+    sm.time[s] = t;
+    sm.ref[s] = r;
+    sm.blo[s] = lo;
+    sm.bhi[s] = hi;
+  }
+  for (int w = threadIdx.x; w < nwords; w += blockDim.x) sm.dirty[w] = 0u;
+  if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = sm.ctr[2] = sm.ctr[3] = 0u;
+  cluster.sync();
+  cx.tick(3);
+
+  bool first = true, worked = false;
+  int par = 0;
+  for (;;) {
+    ++cx.sweeps;
+    // ---- evaluate: this CTA's list (all its tile cells, or its marks) ----
+    if (first) {
+      for (int s0 = (int)(threadIdx.x & ~31u); s0 < nslots; s0 += blockDim.x) {
+        const int s = s0 + (int)lane;
+        bool in_tile = false;
+        if (s < nslots) {
+          const int hx = s % g.P, hy = g.rank + (s / g.P) * g.C;
+          in_tile = hx >= 1 && hx <= g.TW && hy >= 1 && hy <= g.TH;
+        }
+        const uint32_t at = warp_append(sm.ctr + 0, in_tile ? 1u : 0u, lane);
+        if (in_tile) sm.list[at] = (uint16_t)s;
+      }
+    } else {
+      for (int w0 = (int)(threadIdx.x & ~31u); w0 < nwords; w0 += blockDim.x) {
+        const int w = w0 + (int)lane;
+        uint32_t bits = 0;
+        if (w < nwords) {
+          bits = sm.dirty[w];
+          if (bits) sm.dirty[w] = 0u;
+        }
+        uint32_t at = warp_append(sm.ctr + 0, __popc(bits), lane);
+        for (; bits; bits &= bits - 1) sm.list[at++] = (uint16_t)(w * 32 + __ffs(bits) - 1);
+      }
+    }
+    __syncthreads();
+    const uint32_t nlist = sm.ctr[0];
+    if (threadIdx.x == 0) cx.cnt.evals += nlist;
+    for (uint32_t base = threadIdx.x & ~31u; base < nlist; base += blockDim.x) {
+      const uint32_t i = base + lane;
+      bool improved = false;
+      Best b{0.0f, 0u};
+      uint32_t s = 0;
+      if (i < nlist) {
+        s = sm.list[i];
+        const int hx = (int)s % g.P, hy = g.rank + ((int)s / g.P) * g.C;
+        b = evaluate_smem(j, dc, sm, g, hx, hy, cx.cnt);
+        improved = b.time < sm.time[s];
+      }
+      const uint32_t at = warp_append(sm.ctr + 1, improved ? 1u : 0u, lane);
+      if (improved) {
+        sm.uidx[at] = (uint16_t)s;
+        sm.utime[at] = b.time;
+        sm.uref[at] = b.ref;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && sm.ctr[1]) atomicAdd(rank_ptr(sm.ctr, 0) + 2 + par, sm.ctr[1]);
+    cluster.sync();
+    cx.tick(first ? 0 : 1);
+    const uint32_t total = rank_ptr(sm.ctr, 0)[2 + par];
+    if (total == 0) break;
+    worked = true;
+    // ---- commit, mark, referrer scans (scans may run concurrently with
+    // the commits of the same sweep: see tile_global) ----
+    if (cx.leader) {
+      sm.ctr[2 + (par ^ 1)] = 0u;  // the next sweep's cluster counter
+      cx.improvements += total;
+    }
+    const uint32_t nupd = sm.ctr[1];
+    for (uint32_t base = threadIdx.x & ~31u; base < nupd; base += blockDim.x) {
+      const uint32_t u = base + lane;
+      const bool valid = u < nupd;
+      uint32_t want = 0;
+      Box box{1, 1, 0, 0};
+      if (valid) {
+        const uint32_t s = sm.uidx[u];
+        const int hx = (int)s % g.P, hy = g.rank + ((int)s / g.P) * g.C;
+        const int x = g.x0 - 1 + hx, y = g.y0 - 1 + hy;
+        const uint32_t r = sm.uref[u];
+        sm.time[s] = sm.utime[u];
+        sm.ref[s] = r;
+        // referrer box of r: in shared memory inside the staged region, else
+        // in global memory
+        const int rhx = ref_x(r) - (g.x0 - 1), rhy = ref_y(r) - (g.y0 - 1);
+        if (rhx >= 0 && rhy >= 0 && rhx < g.P && rhy < g.HR) {
+          const int owner = rhy % g.C;
+          const int li = (rhy / g.C) * g.P + rhx;
+          smem_box_cas((owner == g.rank ? sm.blo : rank_ptr(sm.blo, owner)) + li, x, y, true);
+          smem_box_cas((owner == g.rank ? sm.bhi : rank_ptr(sm.bhi, owner)) + li, x, y, false);
+        } else {
+          box_expand_global(j, r, x, y);
+        }
+        mark3x3_smem(sm, g, hx, hy);
+        want = pack_ref(x, y);
+        const uint32_t lo = sm.blo[s];
+        if (lo != kEmptyBox) {
+          const uint32_t hi = sm.bhi[s];
+          box = clip_box((int)(lo & 0xFFFFu), (int)(lo >> 16), (int)(hi & 0xFFFFu), (int)(hi >> 16),
+                         g.x0, g.y0, g.TW, g.TH, j.W, j.H);
+        }
+      }
+      warp_scan_boxes(
+          scan_boxes + (threadIdx.x & ~31u), box, want, lane, cx.cnt,
+          [&](int xx, int yy, float &t) {
+            uint32_t r;
+            smem_cell(sm, g, xx - (g.x0 - 1), yy - (g.y0 - 1), t, r);
+            return r;
+          },
+          [&](bool hit, int xx, int yy) {
+            if (hit) mark3x3_smem(sm, g, xx - (g.x0 - 1), yy - (g.y0 - 1));
+          });
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = 0u;
+    cluster.sync();
+    cx.tick(2);
+    par ^= 1;
+    first = false;
+    if (cx.sweeps > cx.max_sweeps) {
+      cx.abort = true;
+      break;
+    }
+  }
+  // ---- write the tile and its halo back (halo times and references are
+  // unchanged; their referrer boxes may have grown) ----
+  for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
+    const int lr = s / g.P, hx = s % g.P;
+    const int hy = g.rank + lr * g.C;
+    const int gx = g.x0 - 1 + hx, gy = g.y0 - 1 + hy;
+    if (gx < 0 || gy < 0 || gx >= j.W || gy >= j.H) continue;
+    const int64_t c = gx + (int64_t)gy * j.W;
+    j.time[c] = sm.time[s];
+    j.refs[c] = sm.ref[s];
+    const uint32_t lo = sm.blo[s];
+    if (lo != kEmptyBox) {
+      const uint32_t hi = sm.bhi[s];
+      j.box_x0[c] = lo & 0xFFFFu;
+      j.box_y0[c] = lo >> 16;
+      j.box_x1[c] = hi & 0xFFFFu;
+      j.box_y1[c] = hi >> 16;
+    }
+  }
+  if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = 0u;
+  sync_cluster();
+  cx.tick(3);
+  return worked;
+}
+
+// ================================================================ engine ====
 __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev *__restrict__ jobs,
                                                          uint32_t n_jobs,
                                                          const SlotDev *__restrict__ slots,
                                                          uint32_t *__restrict__ queue,
                                                          StatsDev *__restrict__ stats,
                                                          unsigned long long max_sweeps) {
+  extern __shared__ __align__(16) char dyn_smem[];
   cg::cluster_group cluster = cg::this_cluster();
   const uint32_t csize = cluster.num_blocks();
   const uint32_t slot_id = blockIdx.x / csize;
@@ -328,14 +819,12 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
   const uint32_t nthreads = csize * blockDim.x;
   const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t gwarp = tid >> 5;
-  const bool leader = tid == 0;
   __shared__ DirConst dc;
   __shared__ JobDev js;
   __shared__ ScanBox scan_boxes[kEngineThreads];
 
   for (;;) {
-    if (leader) {
+    if (tid == 0) {
       s.ctr[4] = atomicAdd(queue, 1u);
       s.ctr[0] = s.ctr[1] = s.ctr[2] = s.ctr[3] = 0;
     }
@@ -349,159 +838,54 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
     __syncthreads();
     const JobDev &j = js;  // shared-memory copy: frees registers
     StatsDev *st = stats + jid;
-    uint32_t dda = 0, gat = 0, walk_max = 0;
-    unsigned long long rounds = 0, launches = 0, sweeps = 0, evals = 0, improvements = 0,
-                       scans = 0;
-    unsigned long long cyc[3] = {0, 0, 0};  // first sweeps, evaluate, commit
-    long long t_phase = clock64();
-    bool abort = false;
+    SweepCtx cx;
+    cx.leader = tid == 0;
+    cx.max_sweeps = max_sweeps;
+    cx.t_phase = clock64();
+    unsigned long long rounds = 0, launches = 0;
     for (;;) {  // rounds
       ++rounds;
       bool round_worked = false;
-      for (int t = 0; t < j.TX * j.TY && !abort; ++t) {  // tiles, row-major
+      for (int t = 0; t < j.TX * j.TY && !cx.abort; ++t) {  // tiles, row-major
         ++launches;
-        const int x0 = (t % j.TX) * j.T, y0 = (t / j.TX) * j.T;
-        const int TW = min(j.T, j.W - x0), TH = min(j.T, j.H - y0);
-        const uint32_t TN = (uint32_t)TW * (uint32_t)TH;
-        bool first = true;
-        int p = 0;
-        for (;;) {  // sweeps
-          // ---- evaluate (Jacobi: nothing is written to the state) ----
-          const uint32_t nitems = first ? TN : __ldcg(s.ctr + p);
-          ++sweeps;  // every thread counts, so the abort below is uniform
-          if (leader) {
-            s.ctr[p ^ 1] = 0;
-            evals += nitems;
-          }
-          for (uint32_t base = gwarp * 32; base < nitems; base += nthreads) {
-            const uint32_t i = base + lane;
-            bool improved = false;
-            Best b{0.0f, 0u};
-            uint32_t k = i;
-            if (i < nitems) {
-              if (!first) {
-                k = __ldcg(s.cand[p] + i);
-                atomicAnd(s.dirty + (k >> 5), ~(1u << (k & 31)));
-              }
-              const int x = x0 + (int)(k % (uint32_t)TW), y = y0 + (int)(k / (uint32_t)TW);
-              b = evaluate(j, dc, x, y, dda, gat, walk_max);
-              improved = b.time < __ldcg(j.time + x + (int64_t)y * j.W);
-            }
-            const uint32_t at = warp_append(s.ctr + 2, improved ? 1u : 0u, lane);
-            if (improved) s.upd[at] = Update{k, b.time, b.ref, 0u};
-          }
-          sync_cluster();
-          if (leader) {
-            const long long now = clock64();
-            cyc[first ? 0 : 1] += (unsigned long long)(now - t_phase);
-            t_phase = now;
-          }
-          const uint32_t nupd = __ldcg(s.ctr + 2);
-          if (nupd == 0) break;
-          round_worked = true;
-          // ---- commit (update_point / commit_point), mark, referrer scans ----
-          // A referrer scan may run while other cells of this sweep commit: a
-          // cell whose reference changes in this sweep is itself marked, and a
-          // box only grows, so what the scan must find (referrers from earlier
-          // sweeps) is unaffected by the concurrent writes.
-          for (uint32_t base = gwarp * 32; base < nupd; base += nthreads) {
-            const uint32_t u = base + lane;
-            const bool valid = u < nupd;
-            int lx = 0, ly = 0;
-            uint32_t c = 0;
-            Box box{1, 1, 0, 0};
-            if (valid) {
-              const Update up = s.upd[u];
-              lx = (int)(up.k % (uint32_t)TW);
-              ly = (int)(up.k / (uint32_t)TW);
-              const int x = x0 + lx, y = y0 + ly;
-              c = (uint32_t)(x + y * j.W);
-              j.time[c] = up.time;
-              j.refs[c] = up.ref;
-              const int64_t rc = ref_x(up.ref) + (int64_t)ref_y(up.ref) * j.W;
-              box_min(j.box_lo + rc, x, y);
-              box_max(j.box_hi + rc, x, y);
-              if (__ldcg(j.box_lo + c) != 0xFFFFFFFFu) box = clipped_box(j, c, x0, y0, TW, TH);
-            }
-            mark3x3(s, p ^ 1, valid, lx, ly, TW, TH, lane);
-            // referrer scans: the warp walks the concatenation of its lanes'
-            // boxes, 32 cells per step, one independent load wave per step
-            const uint32_t area = box.area();
-            scans += area ? 1 : 0;
-            uint32_t incl = area;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-              const uint32_t v = __shfl_up_sync(kFull, incl, o);
-              if (lane >= (uint32_t)o) incl += v;
-            }
-            const uint32_t total = __shfl_sync(kFull, incl, 31);
-            if (total == 0) continue;
-            ScanBox *sb = scan_boxes + (threadIdx.x & ~31u);
-            sb[lane] = ScanBox{box.x0, box.y0, (uint32_t)max(box.x1 - box.x0 + 1, 1),
-                               pack_ref((int)(c % (uint32_t)j.W), (int)(c / (uint32_t)j.W)), incl};
-            __syncwarp();
-            for (uint32_t q0 = 0; q0 < total; q0 += 32) {
-              const uint32_t q = q0 + lane;
-              bool hit = false;
-              int xx = 0, yy = 0;
-              if (q < total) {
-                int lo = 0, hi = 31;  // first lane whose inclusive end exceeds q
-                while (lo < hi) {
-                  const int mid = (lo + hi) >> 1;
-                  if (sb[mid].incl > q) hi = mid; else lo = mid + 1;
-                }
-                const ScanBox o = sb[lo];
-                const uint32_t a = q - (lo ? sb[lo - 1].incl : 0u);  // offset in lane lo's box
-                xx = o.x0 + (int)(a % o.bw);
-                yy = o.y0 + (int)(a / o.bw);
-                hit = refers(j, xx, yy, o.want);
-              }
-              if (__any_sync(kFull, hit)) mark3x3(s, p ^ 1, hit, xx - x0, yy - y0, TW, TH, lane);
-            }
-            __syncwarp();
-          }
-          sync_cluster();
-          if (leader) {
-            const long long now = clock64();
-            cyc[2] += (unsigned long long)(now - t_phase);
-            t_phase = now;
-            improvements += nupd;
-            s.ctr[2] = 0;  // the update list was consumed
-          }
-          p ^= 1;
-          first = false;
-          if (sweeps > max_sweeps) {
-            abort = true;
-            break;
-          }
-        }
+        TileDesc td;
+        td.x0 = (t % j.TX) * j.T;
+        td.y0 = (t / j.TX) * j.T;
+        td.TW = min(j.T, j.W - td.x0);
+        td.TH = min(j.T, j.H - td.y0);
+        const bool w = j.smem_tile ? tile_smem(j, dc, dyn_smem, td, scan_boxes, cx)
+                                   : tile_global(j, dc, s, td, scan_boxes, tid, nthreads, cx);
+        round_worked |= w;
       }
-      if (!round_worked || abort) break;
+      if (!round_worked || cx.abort) break;
     }
     // per-job statistics
+    Counters &cnt = cx.cnt;
+    unsigned long long evals = cnt.evals, scans = cnt.scans;
     for (int o = 16; o > 0; o >>= 1) {
-      dda += __shfl_xor_sync(kFull, dda, o);
-      gat += __shfl_xor_sync(kFull, gat, o);
-      walk_max = max(walk_max, __shfl_xor_sync(kFull, walk_max, o));
+      cnt.dda += __shfl_xor_sync(kFull, cnt.dda, o);
+      cnt.gat += __shfl_xor_sync(kFull, cnt.gat, o);
+      cnt.walk_max = max(cnt.walk_max, __shfl_xor_sync(kFull, cnt.walk_max, o));
       scans += __shfl_xor_sync(kFull, scans, o);
+      evals += __shfl_xor_sync(kFull, evals, o);
     }
     if (lane == 0) {
-      if (dda) atomicAdd(&st->dda_steps, (unsigned long long)dda);
-      if (gat) atomicAdd(&st->gathers, (unsigned long long)gat);
+      if (cnt.dda) atomicAdd(&st->dda_steps, (unsigned long long)cnt.dda);
+      if (cnt.gat) atomicAdd(&st->gathers, (unsigned long long)cnt.gat);
       if (scans) atomicAdd(&st->refbox_scans, scans);
-      if (walk_max) atomicMax(&st->max_walk, walk_max);
+      if (evals) atomicAdd(&st->evaluations, evals);
+      if (cnt.walk_max) atomicMax(&st->max_walk, cnt.walk_max);
     }
-    if (leader) {
+    if (cx.leader) {
       st->rounds = rounds;
       st->launches = launches;
-      st->sweeps = sweeps;
-      st->evaluations = evals;
-      st->improvements = improvements;
-      st->cyc_first = cyc[0];
-      st->cyc_eval = cyc[1];
-      st->cyc_commit = cyc[2];
-      st->cyc_scan = 0;
-      if (abort) st->status = kStatusSweepLimit;
+      st->sweeps = cx.sweeps;
+      st->improvements = cx.improvements;
+      st->cyc_first = cx.cyc[0];
+      st->cyc_eval = cx.cyc[1];
+      st->cyc_commit = cx.cyc[2];
+      st->cyc_stage = cx.cyc[3];
+      if (cx.abort) st->status = kStatusSweepLimit;
     }
     sync_cluster();
   }
@@ -526,15 +910,11 @@ __global__ void __launch_bounds__(256) post_kernel(const JobDev *__restrict__ jo
     if (j.out_rx) j.out_rx[i] = (uint16_t)(r & 0xFFFFu);
     if (j.out_ry) j.out_ry[i] = (uint16_t)(r >> 16);
   }
-  for (int o = 16; o > 0; o >>= 1) burned += __shfl_xor_sync(0xFFFFFFFFu, burned, o);
+  for (int o = 16; o > 0; o >>= 1) burned += __shfl_xor_sync(kFull, burned, o);
   if ((threadIdx.x & 31) == 0 && burned) atomicAdd(&stats[blockIdx.y].burned, burned);
 }
 
-}  // namespace propag
-
 // ------------------------------------------------------------ launchers ----
-namespace propag {
-
 static unsigned grid_for(uint64_t cells, int sms) {
   uint64_t blocks = (cells + 255) / 256;
   const uint64_t cap = (uint64_t)sms * 8;
@@ -554,12 +934,12 @@ cudaError_t launch_ignite(const JobDev *jobs, uint32_t n_jobs, cudaStream_t stre
   return cudaGetLastError();
 }
 
-static cudaLaunchConfig_t engine_config(int csize, int threads, unsigned blocks,
+static cudaLaunchConfig_t engine_config(int csize, int threads, unsigned blocks, size_t smem,
                                         cudaLaunchAttribute *attr, cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks, 1, 1);
   cfg.blockDim = dim3(threads, 1, 1);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = stream;
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = csize;
@@ -570,21 +950,29 @@ static cudaLaunchConfig_t engine_config(int csize, int threads, unsigned blocks,
   return cfg;
 }
 
-cudaError_t engine_max_clusters(int csize, int threads, int *n) {
+static cudaError_t engine_attrs(size_t smem) {
   cudaError_t e = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+int engine_threads() { return kEngineThreads; }
+
+cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n) {
+  cudaError_t e = engine_attrs(smem);
+  if (e != cudaSuccess) return e;
   cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = engine_config(csize, threads, (unsigned)csize, attr, 0);
+  cudaLaunchConfig_t cfg = engine_config(csize, threads, (unsigned)csize, smem, attr, 0);
   return cudaOccupancyMaxActiveClusters(n, engine_kernel, &cfg);
 }
 
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
-                          uint32_t n_slots, int csize, int threads, uint32_t *queue,
+                          uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
                           StatsDev *stats, unsigned long long max_sweeps, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaError_t e = engine_attrs(smem);
   if (e != cudaSuccess) return e;
   cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = engine_config(csize, threads, n_slots * (unsigned)csize, attr, stream);
+  cudaLaunchConfig_t cfg = engine_config(csize, threads, n_slots * (unsigned)csize, smem, attr, stream);
   return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps);
 }
 

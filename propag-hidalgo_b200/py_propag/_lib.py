@@ -108,7 +108,7 @@ class PropagOptions(C.Structure):
 
 STAT_FIELDS = ("rounds", "launches", "sweeps", "evaluations", "improvements", "dda_steps",
                "refbox_scans", "burned", "gathers", "cyc_first", "cyc_eval", "cyc_commit",
-               "cyc_scan")
+               "cyc_stage")
 
 
 class PropagStats(C.Structure):

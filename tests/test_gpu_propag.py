@@ -73,6 +73,24 @@ def test_ridges_lakes_roads_many_ignitions(pp, oracle, tile):
     assert res.stats["improvements"] > 0
 
 
+@pytest.mark.parametrize("cluster", [1, 2, 16])
+def test_shared_memory_and_global_tiles(pp, oracle, cluster):
+    """The same scenario with the tile resident in the cluster's shared
+    memory (when it fits) and in global memory (cluster 1 cannot hold a
+    130 x 130 halo'd tile): both bit-exact against the restatement."""
+    from py_propag import scenarios as S
+    sc = S.config1(size=128, seed=5, n_ign=4, max_time=10000.0)
+    s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
+    res = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=-1, cluster=cluster)
+    sp, az, ec = _fire(pp, sc.terrain)
+    o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                         sc.ignitions, tile=0)
+    assert np.array_equal(res.arrival_times.view(np.uint32), o.time.view(np.uint32))
+    assert np.array_equal(res.refs_x.reshape(sc.height, sc.width), o.refs_x)
+    for k in ("sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
+        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+
+
 def test_north_up_and_staggered_ignition_times(pp, oracle):
     from py_propag import scenarios as S
     sc = S.config0(size=96, seed=4)
