@@ -328,10 +328,13 @@ typedef struct {
   uint16_t x0, y0, x1, y1; /* empty when x0 > x1 */
 } box_t;
 
+/* Marks the eight neighbours of tile cell (lx, ly) (a cell's own change does
+ * not change its own evaluation). */
 static inline void mark(uint8_t *dirty, int32_t *cand, int64_t *ncand, int TW, int TH, int lx,
                         int ly) {
   for (int j = -1; j < 2; j++)
     for (int i = -1; i < 2; i++) {
+      if (i == 0 && j == 0) continue;
       int ax = lx + i, ay = ly + j;
       if (ax < 0 || ay < 0 || ax >= TW || ay >= TH) continue;
       int32_t kk = ax + ay * TW;
@@ -358,14 +361,17 @@ static int run_tile(world_t *w, box_t *refbox, int x0, int y0, int x1, int y1, i
     if (full || first) {
       for (int64_t k = 0; k < TN; k++) cand[ncand++] = (int32_t)k;
     } else {
-      /* cells whose inputs changed: the 3x3 of every changed cell, and the 3x3
-       * of every cell whose reference changed (found through the box of cells
-       * that ever adopted that reference) */
+      /* cells whose inputs changed: the neighbours of every changed cell that
+       * burns (a cell that does not burn is skipped by its neighbours), and
+       * the neighbours of every burning cell whose reference changed (found
+       * through the box of cells that ever adopted that reference) */
       for (int64_t c = 0; c < nchg; c++) {
         int32_t k = chg[c];
         int lx = k % TW, ly = k / TW;
-        mark(dirty, cand, &ncand, TW, TH, lx, ly);
         const int gx = x0 + lx, gy = y0 + ly;
+        const int64_t gc = (int64_t)gx + (int64_t)gy * W;
+        if (w->time[gc] < w->s->max_time && w->speed[gc] != 0.0f)
+          mark(dirty, cand, &ncand, TW, TH, lx, ly);
         const box_t b = refbox[(int64_t)gx + (int64_t)gy * W];
         if (b.x0 > b.x1) continue;
         stats[7]++;
@@ -381,15 +387,16 @@ static int run_tile(world_t *w, box_t *refbox, int x0, int y0, int x1, int y1, i
           for (int xx = bx0; xx <= bx1; xx++) {
             const int64_t n = (int64_t)xx + (int64_t)yy * W;
             stats[8]++;
-            if (w->time[n] < FLT_MAX && w->rx[n] == (uint16_t)gx && w->ry[n] == (uint16_t)gy)
+            if (w->time[n] < w->s->max_time && w->speed[n] != 0.0f && w->rx[n] == (uint16_t)gx &&
+                w->ry[n] == (uint16_t)gy)
               mark(dirty, cand, &ncand, TW, TH, xx - x0, yy - y0);
           }
       }
       for (int64_t c = 0; c < ncand; c++) dirty[cand[c]] = 0;
     }
-    if (ncand == 0) break;
-    first = 0;
     stats[2]++;
+    if (ncand == 0) break; /* the reference's final sweep, which improves nothing */
+    first = 0;
     stats[3] += ncand;
     /* evaluate (Jacobi: all reads see the previous sweep's state) */
     int64_t dda = 0, gat = 0;

@@ -155,45 +155,104 @@ struct Counters {
   unsigned long long evals = 0, scans = 0;
 };
 
-// find_neighbor_which_reaches_first (propag.cu:124-190) given the already
-// fetched state of the eight neighbours: nt (times), fs/fa/fe (fire), nr
-// (references), rt (times of the references), act (bit k: neighbour k is
-// burning, in the grid and not referencing the cell).  Runs the reference's
-// sequential decision logic over the neighbours in its order, in registers.
-__device__ __forceinline__ Best decide(const JobDev &j, const DirConst &dc, int x, int y,
-                                       Best best, const float nt[8], const float fs[8],
-                                       const float fa[8], const float fe[8], const uint32_t nr[8],
-                                       const float rt[8], uint32_t act, Counters &cnt) {
-  const bool nu = j.north_up != 0;
-  cnt.gat += __popc(act);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    if (!((act >> k) & 1u)) continue;
-    const int kk = k < 4 ? k : k + 1;
-    const int nx = x + kk % 3 - 1, ny = y + kk / 3 - 1;
-    const int rx = ref_x(nr[k]), ry = ref_y(nr[k]);
-    const Fire f{fs[k], fa[k], fe[k]};
-    const float ntime = step_time(nt[k], dc.dist[k], __fmul_rn(f.speed_max, spread_factor(dc.bearing[k], f)));
-    float cand = time_from(rx, ry, rt[k], x, y, f, j.gdx, j.gdy, nu);
-    if (cand < ntime && cand < best.time) {
-      uint32_t cref = nr[k];
-      const uint32_t before = cnt.dda;
-      const bool blocked = line_blocked_call(j.bnd, j.W, nx, ny, rx, ry, cnt.dda);
-      cnt.walk_max = max(cnt.walk_max, cnt.dda - before);
-      if (blocked) {
-        cref = pack_ref(nx, ny);
-        cand = ntime;
-      }
-      if (cand < best.time) {
-        best.time = cand;
-        best.ref = cref;
-      }
-    } else if (ntime < best.time) {
-      best.time = ntime;
-      best.ref = pack_ref(nx, ny);
+// find_neighbor_which_reaches_first (propag.cu:124-190) evaluated by the 8
+// lanes of a lane group (lanes 8c .. 8c+7), lane k taking neighbour k in the
+// reference's order.  Every neighbour offers a time that does not depend on
+// the best found so far -- the candidate through its reference, or its own
+// direct time when the line of sight is blocked or the candidate is not
+// faster -- and the sequential loop keeps the first strictly smaller offer;
+// so the result is the first minimum of the offers when it beats the cell's
+// own time.  A lane walks its line of sight whenever the sequential loop
+// could (candidate faster than the neighbour's direct time and than the
+// cell's own time); only the walks the sequential loop performs (candidate
+// also faster than every earlier offer) are counted, so the counters match
+// the reference's order exactly.  Called by all 32 lanes.
+struct GlobalAcc {
+  const JobDev &j;
+  __device__ __forceinline__ void cell(int x, int y, float &t, uint32_t &r) const {
+    const int64_t n = x + (int64_t)y * j.W;
+    t = __ldcg(j.time + n);
+    r = __ldcg(j.refs + n);
+  }
+  __device__ __forceinline__ float time_of(uint32_t r) const {
+    return __ldcg(j.time + ref_x(r) + (int64_t)ref_y(r) * j.W);
+  }
+};
+
+template <typename Acc>
+__device__ __forceinline__ Best evaluate_coop(const JobDev &j, const DirConst &dc, const Acc &acc,
+                                              int x, int y, Best own, bool valid, uint32_t lane,
+                                              Counters &cnt) {
+  const float kInf = __int_as_float(0x7f800000);
+  const int k = (int)(lane & 7u);
+  const int kk = k < 4 ? k : k + 1;
+  const int nx = x + kk % 3 - 1, ny = y + kk / 3 - 1;
+  bool act = false;
+  float nt = FLT_MAX, rt = FLT_MAX;
+  uint32_t nr = kNoRef;
+  Fire f{0.0f, 0.0f, 0.0f};
+  if (valid && nx >= 0 && ny >= 0 && nx < j.W && ny < j.H) {
+    acc.cell(nx, ny, nt, nr);
+    const int64_t n = nx + (int64_t)ny * j.W;
+    f.speed_max = __ldg(j.speed + n);
+    act = nt < j.max_time && f.speed_max != 0.0f && !(ref_x(nr) == x && ref_y(nr) == y);
+    if (act) {
+      f.azimuth_max = __ldg(j.az + n);
+      f.eccentricity = __ldg(j.ecc + n);
+      rt = acc.time_of(nr);
     }
   }
-  return best;
+  cnt.gat += act ? 1u : 0u;
+  float offer = kInf, cand = kInf;
+  uint32_t oref = 0, steps = 0;
+  bool walked = false;
+  if (act) {
+    const float ntime =
+        step_time(nt, dc.dist[k], __fmul_rn(f.speed_max, spread_factor(dc.bearing[k], f)));
+    cand = time_from(ref_x(nr), ref_y(nr), rt, x, y, f, j.gdx, j.gdy, j.north_up != 0);
+    offer = ntime;
+    oref = pack_ref(nx, ny);
+    if (cand < ntime) {
+      bool blocked = false;
+      if (cand < own.time) {
+        walked = true;
+        blocked = line_blocked_call(j.bnd, j.W, nx, ny, ref_x(nr), ref_y(nr), steps);
+      }
+      if (!blocked) {
+        offer = cand;
+        oref = nr;
+      }
+    }
+  }
+  // running best of the sequential loop before neighbour k (exclusive min)
+  float pm = offer;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    const float t = __shfl_up_sync(kFull, pm, o);
+    if (k >= o && t < pm) pm = t;
+  }
+  float before = __shfl_up_sync(kFull, pm, 1);
+  if (k == 0) before = kInf;
+  if (walked && cand < before) {
+    cnt.dda += steps;
+    cnt.walk_max = max(cnt.walk_max, steps);
+  }
+  // first minimum of the offers
+  float bv = offer;
+  uint32_t br = oref;
+  int bi = k;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    const float ov = __shfl_xor_sync(kFull, bv, o);
+    const uint32_t orf = __shfl_xor_sync(kFull, br, o);
+    const int oi = __shfl_xor_sync(kFull, bi, o);
+    if (ov < bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      br = orf;
+      bi = oi;
+    }
+  }
+  return bv < own.time ? Best{bv, br} : own;
 }
 
 // Warp-aggregated append: every lane of the (fully active) warp passes its
@@ -252,7 +311,8 @@ struct ScanBox {
 // time.
 template <typename RefFn, typename MarkFn>
 __device__ __forceinline__ void warp_scan_boxes(ScanBox *sb, const Box &box, uint32_t want,
-                                                uint32_t lane, Counters &cnt, RefFn ref_fn,
+                                                const JobDev &j, uint32_t lane, Counters &cnt,
+                                                RefFn ref_fn,
                                                 MarkFn mark_fn) {
   const uint32_t area = box.area();
   cnt.scans += area ? 1 : 0;
@@ -277,7 +337,10 @@ __device__ __forceinline__ void warp_scan_boxes(ScanBox *sb, const Box &box, uin
       yy = o.y0 + (int)(a / o.bw);
       float t;
       const uint32_t r = ref_fn(xx, yy, t);
-      hit = r == o.want && t < FLT_MAX;
+      // a referrer that burns (a cell that does not burn is skipped by its
+      // neighbours; requiring it makes the marked set independent of the
+      // order of this sweep's commits)
+      hit = r == o.want && t < j.max_time && __ldg(j.speed + xx + (int64_t)yy * j.W) != 0.0f;
     }
     mark_fn(hit, xx, yy);
   }
@@ -304,44 +367,6 @@ struct TileDesc {
 };
 
 // ================================================ global-memory tiles ====
-__device__ __forceinline__ Best evaluate_global(const JobDev &j, const DirConst &dc, int x, int y,
-                                                Counters &cnt) {
-  const int W = j.W, H = j.H;
-  const int64_t me = x + (int64_t)y * W;
-  Best best{__ldcg(j.time + me), __ldcg(j.refs + me)};
-  float nt[8], rt[8], fs[8], fa[8], fe[8];
-  uint32_t nr[8];
-  uint32_t act = 0;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int kk = k < 4 ? k : k + 1;
-    const int nx = x + kk % 3 - 1, ny = y + kk / 3 - 1;
-    const bool inb = nx >= 0 && ny >= 0 && nx < W && ny < H;
-    const int64_t n = nx + (int64_t)ny * W;
-    nt[k] = inb ? __ldcg(j.time + n) : FLT_MAX;
-    fs[k] = inb ? __ldg(j.speed + n) : 0.0f;
-  }
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    if (nt[k] < j.max_time && fs[k] != 0.0f) act |= 1u << k;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int kk = k < 4 ? k : k + 1;
-    const int64_t n = (x + kk % 3 - 1) + (int64_t)(y + kk / 3 - 1) * W;
-    const bool a = (act >> k) & 1u;
-    nr[k] = a ? __ldcg(j.refs + n) : kNoRef;
-    fa[k] = a ? __ldg(j.az + n) : 0.0f;
-    fe[k] = a ? __ldg(j.ecc + n) : 0.0f;
-  }
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    if (ref_x(nr[k]) == x && ref_y(nr[k]) == y) act &= ~(1u << k);  // its reference is me
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    rt[k] = (act >> k) & 1u ? __ldcg(j.time + ref_x(nr[k]) + (int64_t)ref_y(nr[k]) * W) : FLT_MAX;
-  return decide(j, dc, x, y, best, nt, fs, fa, fe, nr, rt, act, cnt);
-}
-
 // Marks the 3x3 neighbourhood of tile cell (lx, ly) for the next sweep
 // (deduplicated through the dirty bitmap) and appends the new cells to work
 // list q.  Called by every lane of a warp; `active` selects the lanes.
@@ -352,7 +377,7 @@ __device__ __forceinline__ void mark3x3_list(const SlotDev &s, int q, bool activ
 #pragma unroll
     for (int t = 0; t < 9; ++t) {
       const int ax = lx + t % 3 - 1, ay = ly + t / 3 - 1;
-      if (ax < 0 || ay < 0 || ax >= TW || ay >= TH) continue;
+      if (t == 4 || ax < 0 || ay < 0 || ax >= TW || ay >= TH) continue;
       const uint32_t k = (uint32_t)ax + (uint32_t)ay * (uint32_t)TW;
       const uint32_t bit = 1u << (k & 31);
       if (!(atomicOr(s.dirty + (k >> 5), bit) & bit)) fresh |= 1u << t;
@@ -401,20 +426,25 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
       s.ctr[p ^ 1] = 0;
       cx.cnt.evals += nitems;
     }
-    for (uint32_t base = gwarp * 32; base < nitems; base += nthreads) {
-      const uint32_t i = base + lane;
-      bool improved = false;
-      Best b{0.0f, 0u};
-      uint32_t k = i;
-      if (i < nitems) {
+    // four cells per warp, eight lanes per cell
+    for (uint32_t base = gwarp * 4; base < nitems; base += (nthreads >> 5) * 4) {
+      const uint32_t ci = base + (lane >> 3);
+      const bool valid = ci < nitems;
+      uint32_t k = ci;
+      int x = 0, y = 0;
+      Best own{FLT_MAX, kNoRef};
+      if (valid) {
         if (!first) {
-          k = __ldcg(s.cand[p] + i);
-          atomicAnd(s.dirty + (k >> 5), ~(1u << (k & 31)));
+          k = __ldcg(s.cand[p] + ci);
+          if ((lane & 7) == 0) atomicAnd(s.dirty + (k >> 5), ~(1u << (k & 31)));
         }
-        const int x = x0 + (int)(k % (uint32_t)TW), y = y0 + (int)(k / (uint32_t)TW);
-        b = evaluate_global(j, dc, x, y, cx.cnt);
-        improved = b.time < __ldcg(j.time + x + (int64_t)y * j.W);
+        x = x0 + (int)(k % (uint32_t)TW);
+        y = y0 + (int)(k / (uint32_t)TW);
+        const int64_t c = x + (int64_t)y * j.W;
+        own = Best{__ldcg(j.time + c), __ldcg(j.refs + c)};
       }
+      const Best b = evaluate_coop(j, dc, GlobalAcc{j}, x, y, own, valid, lane, cx.cnt);
+      const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
       const uint32_t at = warp_append(s.ctr + 2, improved ? 1u : 0u, lane);
       if (improved) s.upd[at] = Update{k, b.time, b.ref, 0u};
     }
@@ -433,6 +463,7 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
       const bool valid = u < nupd;
       int lx = 0, ly = 0;
       uint32_t want = 0;
+      bool burning = false;
       Box box{1, 1, 0, 0};
       if (valid) {
         const Update up = s.upd[u];
@@ -442,6 +473,8 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
         const int64_t c = x + (int64_t)y * j.W;
         j.time[c] = up.time;
         j.refs[c] = up.ref;
+        // only a burning cell is read by its neighbours
+        burning = up.time < j.max_time && __ldg(j.speed + c) != 0.0f;
         box_expand_global(j, up.ref, x, y);
         want = pack_ref(x, y);
         const uint32_t bx0 = __ldcg(j.box_x0 + c);
@@ -449,9 +482,9 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
           box = clip_box((int)bx0, (int)__ldcg(j.box_y0 + c), (int)__ldcg(j.box_x1 + c),
                          (int)__ldcg(j.box_y1 + c), x0, y0, TW, TH, j.W, j.H);
       }
-      mark3x3_list(s, p ^ 1, valid, lx, ly, TW, TH, lane);
+      mark3x3_list(s, p ^ 1, burning, lx, ly, TW, TH, lane);
       warp_scan_boxes(
-          scan_boxes + (threadIdx.x & ~31u), box, want, lane, cx.cnt,
+          scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cx.cnt,
           [&](int xx, int yy, float &t) {
             const int64_t n = xx + (int64_t)yy * j.W;
             t = __ldcg(j.time + n);
@@ -539,7 +572,7 @@ __device__ __forceinline__ void mark3x3_smem(const SmemTile &sm, const SmemGeom 
 #pragma unroll
   for (int t = 0; t < 9; ++t) {
     const int ax = hx + t % 3 - 1, ay = hy + t / 3 - 1;
-    if (ax < 1 || ay < 1 || ax > g.TW || ay > g.TH) continue;
+    if (t == 4 || ax < 1 || ay < 1 || ax > g.TW || ay > g.TH) continue;
     const int owner = ay % g.C;
     const uint32_t li = (uint32_t)((ay / g.C) * g.P + ax);
     uint32_t *d = owner == g.rank ? sm.dirty : rank_ptr(sm.dirty, owner);
@@ -571,39 +604,15 @@ __device__ __forceinline__ float smem_time_of(const JobDev &j, const SmemTile &s
   return __ldcg(j.time + ref_x(r) + (int64_t)ref_y(r) * j.W);  // outside: static this launch
 }
 
-__device__ __forceinline__ Best evaluate_smem(const JobDev &j, const DirConst &dc,
-                                              const SmemTile &sm, const SmemGeom &g, int hx,
-                                              int hy, Counters &cnt) {
-  const int x = g.x0 - 1 + hx, y = g.y0 - 1 + hy;
-  Best best;
-  smem_cell(sm, g, hx, hy, best.time, best.ref);
-  float nt[8], rt[8], fs[8], fa[8], fe[8];
-  uint32_t nr[8];
-  uint32_t act = 0;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int kk = k < 4 ? k : k + 1;
-    const int di = kk % 3 - 1, dj = kk / 3 - 1;
-    const int nx = x + di, ny = y + dj;
-    const bool inb = nx >= 0 && ny >= 0 && nx < j.W && ny < j.H;
-    smem_cell(sm, g, hx + di, hy + dj, nt[k], nr[k]);  // outside the grid: FLT_MAX, no reference
-    fs[k] = inb ? __ldg(j.speed + nx + (int64_t)ny * j.W) : 0.0f;
+struct SmemAcc {
+  const JobDev &j;
+  const SmemTile &sm;
+  const SmemGeom &g;
+  __device__ __forceinline__ void cell(int x, int y, float &t, uint32_t &r) const {
+    smem_cell(sm, g, x - (g.x0 - 1), y - (g.y0 - 1), t, r);
   }
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    if (nt[k] < j.max_time && fs[k] != 0.0f && !(ref_x(nr[k]) == x && ref_y(nr[k]) == y))
-      act |= 1u << k;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int kk = k < 4 ? k : k + 1;
-    const int64_t n = (x + kk % 3 - 1) + (int64_t)(y + kk / 3 - 1) * j.W;
-    const bool a = (act >> k) & 1u;
-    fa[k] = a ? __ldg(j.az + n) : 0.0f;
-    fe[k] = a ? __ldg(j.ecc + n) : 0.0f;
-    rt[k] = a ? smem_time_of(j, sm, g, nr[k]) : FLT_MAX;
-  }
-  return decide(j, dc, x, y, best, nt, fs, fa, fe, nr, rt, act, cnt);
-}
+  __device__ __forceinline__ float time_of(uint32_t r) const { return smem_time_of(j, sm, g, r); }
+};
 
 __device__ __forceinline__ void smem_box_cas(uint32_t *w, int x, int y, bool is_min) {
   uint32_t o = *w;
@@ -693,17 +702,22 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
     __syncthreads();
     const uint32_t nlist = sm.ctr[0];
     if (threadIdx.x == 0) cx.cnt.evals += nlist;
-    for (uint32_t base = threadIdx.x & ~31u; base < nlist; base += blockDim.x) {
-      const uint32_t i = base + lane;
-      bool improved = false;
-      Best b{0.0f, 0u};
+    // four cells per warp, eight lanes per cell
+    for (uint32_t base = (threadIdx.x >> 5) * 4; base < nlist; base += (blockDim.x >> 5) * 4) {
+      const uint32_t ci = base + (lane >> 3);
+      const bool valid = ci < nlist;
       uint32_t s = 0;
-      if (i < nlist) {
-        s = sm.list[i];
+      int x = 0, y = 0;
+      Best own{FLT_MAX, kNoRef};
+      if (valid) {
+        s = sm.list[ci];
         const int hx = (int)s % g.P, hy = g.rank + ((int)s / g.P) * g.C;
-        b = evaluate_smem(j, dc, sm, g, hx, hy, cx.cnt);
-        improved = b.time < sm.time[s];
+        x = g.x0 - 1 + hx;
+        y = g.y0 - 1 + hy;
+        own = Best{sm.time[s], sm.ref[s]};
       }
+      const Best b = evaluate_coop(j, dc, SmemAcc{j, sm, g}, x, y, own, valid, lane, cx.cnt);
+      const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
       const uint32_t at = warp_append(sm.ctr + 1, improved ? 1u : 0u, lane);
       if (improved) {
         sm.uidx[at] = (uint16_t)s;
@@ -748,7 +762,9 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
         } else {
           box_expand_global(j, r, x, y);
         }
-        mark3x3_smem(sm, g, hx, hy);
+        // only a burning cell is read by its neighbours
+        if (sm.utime[u] < j.max_time && __ldg(j.speed + x + (int64_t)y * j.W) != 0.0f)
+          mark3x3_smem(sm, g, hx, hy);
         want = pack_ref(x, y);
         const uint32_t lo = sm.blo[s];
         if (lo != kEmptyBox) {
@@ -758,7 +774,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
         }
       }
       warp_scan_boxes(
-          scan_boxes + (threadIdx.x & ~31u), box, want, lane, cx.cnt,
+          scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cx.cnt,
           [&](int xx, int yy, float &t) {
             uint32_t r;
             smem_cell(sm, g, xx - (g.x0 - 1), yy - (g.y0 - 1), t, r);
