@@ -199,3 +199,23 @@ def trig_batch(a, b):
     t = np.zeros_like(a)
     lib.ops_trig_batch(C.c_int64(a.size), _ptr(a), _ptr(b), _ptr(c), _ptr(t))
     return c, t
+
+
+def rounding_batch(x):
+    """(round-down reciprocal, round-toward-zero square root) of float32 x."""
+    lib = _load()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    r = np.zeros_like(x)
+    s = np.zeros_like(x)
+    lib.ops_rounding_batch(C.c_int64(x.size), _ptr(x), _ptr(r), _ptr(s))
+    return r, s
+
+
+def dda_cells(fx, fy, tx, ty):
+    """Cells visited by the line-of-sight walk (propag.h:91-135)."""
+    lib = _load()
+    lib.ops_dda_cells.restype = C.c_int64
+    cap = abs(tx - fx) + abs(ty - fy) + 4
+    out = np.zeros(2 * cap, dtype=np.int32)
+    n = lib.ops_dda_cells(C.c_int(fx), C.c_int(fy), C.c_int(tx), C.c_int(ty), _ptr(out), C.c_int64(cap))
+    return [tuple(p) for p in out[: 2 * min(n, cap)].reshape(-1, 2)]

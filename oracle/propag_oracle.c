@@ -27,10 +27,12 @@
  * Jacobi iteration.
  *
  * Work skipping that keeps results identical: after the first sweep of a
- * launch, a cell is re-evaluated only if one of its 3x3 neighbourhood changed
- * in the previous sweep; if a changed cell is the reference of any cell, the
- * next sweep evaluates the whole tile (a reference's time is read by cells far
- * away, propag.cu:221-224).  `full` = 1 disables the skipping.
+ * launch, a cell is re-evaluated only if one of its inputs changed in the
+ * previous sweep: a burning neighbour changed, or the reference of a burning
+ * neighbour changed (a reference's time is read by cells far away,
+ * propag.cu:221-224; every cell keeps the bounding box of the cells that ever
+ * adopted it as their reference, and that box is scanned).  `full` = 1
+ * evaluates the whole tile in every sweep; the tests check both modes agree.
  *
  * Intrinsics: __frcp_rd and __fsqrt_rz are emulated exactly (round-down
  * reciprocal, round-toward-zero square root).  The cosine and arctangent are
@@ -540,3 +542,53 @@ void ops_trig_batch(int64_t n, const float *a, const float *b, float *cos_out, f
 }
 
 int ops_nstats(void) { return NSTATS; }
+
+/* Exposes the directed-rounding emulation (round-down reciprocal,
+ * round-toward-zero square root) for the tests. */
+void ops_rounding_batch(int64_t n, const float *x, float *rcp_out, float *sqrt_out) {
+  for (int64_t i = 0; i < n; i++) {
+    rcp_out[i] = rcp_rd(x[i]);
+    sqrt_out[i] = x[i] >= 0.0f ? sqrt_rz(x[i]) : NAN;
+  }
+}
+
+/* Visits the cells of the line-of-sight walk from (fx, fy) to (tx, ty) the
+ * way propag.h:91-135 does; writes up to max_out (x, y) pairs and returns the
+ * number of cells visited. */
+int64_t ops_dda_cells(int fx, int fy, int tx, int ty, int32_t *out, int64_t max_out) {
+  int sx = (tx > fx) - (tx < fx), sy = (ty > fy) - (ty < fy);
+  int cx = fx, cy = fy;
+  float tmx = (float)(1.0 / (double)(float)abs(tx - fx));
+  float tmy = (float)(1.0 / (double)(float)abs(ty - fy));
+  const float ddx = tmx, ddy = tmy;
+  int64_t limit = (int64_t)abs(tx - fx) + abs(ty - fy) + 2, k = 0;
+  for (int64_t n = 0; n < limit; n++) {
+    int px = cx, py = cy;
+    if (px == tx && py == ty) {
+      cx += sx;
+      cy += sy;
+    } else {
+      int vx = sx > 0 ? cx <= tx : cx >= tx;
+      int vy = sy > 0 ? cy <= ty : cy >= ty;
+      if (!(vx && vy)) break;
+      if (fabsf(tmx - tmy) < 1e-9f) {
+        cx += sx;
+        cy += sy;
+        tmx += ddx;
+        tmy += ddy;
+      } else if (tmx < tmy) {
+        cx += sx;
+        tmx += ddx;
+      } else {
+        cy += sy;
+        tmy += ddy;
+      }
+    }
+    if (k < max_out) {
+      out[2 * k] = px;
+      out[2 * k + 1] = py;
+    }
+    k++;
+  }
+  return k;
+}
