@@ -170,6 +170,47 @@ int propag_engine_run(propag_engine *engine, const PropagJob *jobs, uint32_t n_j
  * Waits for the last run to finish. */
 int propag_engine_last_times(propag_engine *engine, float ms[3]);
 
+/* Allocation-free propagation of one grid.  No counterpart in the reference:
+ * its propagation allocates its device buffers on every run
+ * (crates/propag/src/propag.rs:420-455).
+ *
+ * Same kernels, schedule and results as propag_engine_run with one job, but
+ * its scratch (references, referrer boxes, boundary bits, job descriptor,
+ * counters, statistics) lives in one fixed device array of about 20.1 MiB,
+ * reserved by the CUDA driver when the library's module holding it is loaded.
+ * The call makes no cudaMalloc, cudaFree or cudaMallocHost, creates no events
+ * and uses no caching allocator.  It is meant for callers that cannot
+ * allocate device memory while they run:
+ *   - a process whose device memory is owned by another allocator (a
+ *     framework's caching pool, or a pool sized at start-up), where a
+ *     cudaMalloc can fail or fragment that pool;
+ *   - a latency-bound serving loop: when a larger job arrives the engine grows
+ *     its scratch (stream synchronise, cudaFree, cudaMalloc), and cudaFree
+ *     waits for the whole device, stalling every other stream;
+ *   - a service that must not fail with out-of-memory after start-up.
+ *
+ * Limits: width * height <= PROPAG_STATIC_MAX_CELLS (1024 x 1024 cells), and
+ * the tile (job->tile; 0 = PROPAG_DEFAULT_TILE, PROPAG_TILE_WHOLE_GRID) with
+ * its one-cell halo must fit in the shared memory of a cluster of at most 16
+ * CTAs (a tile side up to 323 always fits).  Larger jobs are rejected with
+ * PROPAG_ERR_INVALID and a message naming the limit.
+ *
+ * The scratch is one per device.  Calls that overlap on the same device (from
+ * two host threads, or on two streams with no ordering between them) race on
+ * it and corrupt each other's results: serialise them (one stream, or an
+ * event or lock between calls).  Nothing has to be zero beforehand: each call
+ * clears its statistics, job queue and counters and re-initialises the
+ * per-cell state in its own first kernels.  The first call on each device does
+ * set-up (device attributes, the fuel table upload, the scratch's address
+ * through cudaGetSymbolAddress); make that first call outside any stream
+ * capture.
+ *
+ * Stream-ordered: returns once the work is enqueued on `stream`, unless stats
+ * is non-NULL, in which case it synchronises the stream and fills *stats.
+ * The job's pointers are device pointers, as in propag_engine_run. */
+#define PROPAG_STATIC_MAX_CELLS (1u << 20)
+int propag_run_device_static(const PropagJob *job, void *stream, PropagStats *stats);
+
 /* Plain drop-in over host buffers for one grid: fire behaviour (3 fields),
  * boundaries, propagation and post mask, like propagate()
  * (crates/propag/src/propag.rs:323-574) without the file writers.

@@ -19,6 +19,7 @@
 
 #include "engine.cuh"
 #include "io.hpp"
+#include "noalloc.hpp"
 #include "propag_b200.h"
 
 namespace propag {
@@ -393,6 +394,129 @@ extern "C" int propag_engine_last_times(propag_engine *e, float ms[3]) {
   CK(cudaSetDevice(e->device));
   CK(cudaEventSynchronize(e->ev[3]));
   for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms[i], e->ev[i], e->ev[i + 1]));
+  return PROPAG_OK;
+}
+
+// ============================================= allocation-free variant ====
+// One job, the same kernels as engine_run, scratch in the fixed device array
+// of noalloc.cu.  No cudaMalloc/cudaFree/cudaMallocHost, no events, no host
+// heap on the success path.
+namespace propag {
+int engine_threads();  // engine.cu: the engine kernel's launch bound
+}
+static_assert(PROPAG_STATIC_MAX_CELLS == kStaticMaxCells, "header and scratch disagree");
+namespace {
+std::mutex g_static_mu;
+void *g_static_base[64] = {};
+}  // namespace
+
+extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, PropagStats *stats) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (!job) return fail(PROPAG_ERR_INVALID, "null job");
+  const PropagJob &j = *job;
+  if (!valid_size(j.width, j.height)) return fail(PROPAG_ERR_INVALID, "width/height must be 1..65534");
+  const uint64_t N = (uint64_t)j.width * j.height;
+  if (N > kStaticMaxCells)
+    return fail(PROPAG_ERR_INVALID,
+                "propag_run_device_static: grid of " + std::to_string(N) + " cells exceeds its fixed scratch of " +
+                    std::to_string(kStaticMaxCells) + " cells (use propag_engine_run)");
+  if (!j.speed_max || !j.azimuth_max || !j.eccentricity || !j.time)
+    return fail(PROPAG_ERR_INVALID, "null fire/time pointer");
+  if (j.n_ignitions && !j.ignitions) return fail(PROPAG_ERR_INVALID, "null ignitions");
+  if (!(j.dx != 0.0f) || !(j.dy != 0.0f) || !std::isfinite(j.dx) || !std::isfinite(j.dy))
+    return fail(PROPAG_ERR_INVALID, "invalid pixel size");
+  int T = j.tile ? j.tile : PROPAG_DEFAULT_TILE;
+  if (T == PROPAG_TILE_WHOLE_GRID || T <= 0) T = (int)std::max(j.width, j.height);
+  const int tw = std::min<int>(T, (int)j.width), th = std::min<int>(T, (int)j.height);
+  // the smallest cluster whose shared memory holds the tile and its halo
+  const size_t budget = 200 * 1024;
+  int csize = 0;
+  for (int c = 1; c <= 16 && csize == 0; c *= 2)
+    if (smem_bytes(tw, th, c) <= budget) csize = c;
+  if (csize == 0)
+    return fail(PROPAG_ERR_INVALID,
+                "propag_run_device_static: a " + std::to_string(tw) + " x " + std::to_string(th) +
+                    " tile does not fit in a 16-CTA cluster's shared memory (use a tile side <= 323 or "
+                    "propag_engine_run)");
+  const size_t smem = smem_bytes(tw, th, csize);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  char *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_base[dev]) {  // set-up, once per device
+      void *p = nullptr;
+      CK(static_scratch_address(&p));
+      g_static_base[dev] = p;
+    }
+    base = static_cast<char *>(g_static_base[dev]);
+  }
+  int max_clusters = 0;
+  CK(engine_max_clusters(csize, engine_threads(), smem, &max_clusters));
+  if (max_clusters < 1) return fail(PROPAG_ERR_CUDA, "cluster size " + std::to_string(csize) + " cannot be resident");
+  JobDev d{};
+  d.W = (int)j.width;
+  d.H = (int)j.height;
+  d.gdx = j.dx;
+  d.gdy = j.dy;
+  d.max_time = j.max_time;
+  d.T = T;
+  d.TX = (int)((j.width + T - 1) / T);
+  d.TY = (int)((j.height + T - 1) / T);
+  d.north_up = j.dy < 0 ? 1 : 0;
+  d.smem_tile = 1;
+  d.speed = j.speed_max;
+  d.az = j.azimuth_max;
+  d.ecc = j.eccentricity;
+  d.time = j.time;
+  d.ignitions = j.ignitions;
+  d.n_ignitions = j.n_ignitions;
+  d.out_rx = j.refs_x;
+  d.out_ry = j.refs_y;
+  d.out_bnd = j.boundaries;
+  uint32_t *cells = reinterpret_cast<uint32_t *>(base + kStaticCellsOff);
+  d.refs = cells;
+  d.box_x0 = cells + kStaticMaxCells;
+  d.box_y0 = cells + 2 * kStaticMaxCells;
+  d.box_x1 = cells + 3 * kStaticMaxCells;
+  d.box_y1 = cells + 4 * kStaticMaxCells;
+  d.bnd = j.boundaries ? j.boundaries : reinterpret_cast<uint32_t *>(base + kStaticBndOff);
+  SlotDev s{};  // shared-memory tiles use only the counters
+  s.ctr = reinterpret_cast<uint32_t *>(base + kStaticCtrOff);
+  JobDev *d_job = reinterpret_cast<JobDev *>(base + kStaticJobOff);
+  SlotDev *d_slot = reinterpret_cast<SlotDev *>(base + kStaticSlotOff);
+  StatsDev *d_stats = reinterpret_cast<StatsDev *>(base + kStaticStatsOff);
+  uint32_t *d_queue = reinterpret_cast<uint32_t *>(base + kStaticQueueOff);
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  CK(launch_stage_static(d_job, d, d_slot, s, d_stats, d_queue, stream));
+  CK(launch_prep(d_job, 1, N, sms, stream));
+  CK(launch_ignite(d_job, 1, stream));
+  CK(launch_engine(d_job, 1, d_slot, 1, csize, engine_threads(), smem, d_queue, d_stats, 1ull << 40, stream));
+  CK(launch_post(d_job, 1, N, sms, d_stats, stream));
+  if (stats) {
+    StatsDev h;
+    CK(cudaMemcpyAsync(&h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    PropagStats &o = *stats;
+    o.rounds = h.rounds;
+    o.launches = h.launches;
+    o.sweeps = h.sweeps;
+    o.evaluations = h.evaluations;
+    o.improvements = h.improvements;
+    o.dda_steps = h.dda_steps;
+    o.gathers = h.gathers;
+    o.refbox_scans = h.refbox_scans;
+    o.burned = h.burned;
+    o.cyc_first = h.cyc_first;
+    o.cyc_eval = h.cyc_eval;
+    o.cyc_commit = h.cyc_commit;
+    o.cyc_stage = h.cyc_stage;
+    o.status = h.status;
+    o.max_walk = h.max_walk;
+    if (h.status) return fail(PROPAG_ERR_TIMEOUT, "sweep limit reached");
+  }
   return PROPAG_OK;
 }
 

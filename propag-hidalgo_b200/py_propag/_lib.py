@@ -106,6 +106,8 @@ class PropagOptions(C.Structure):
     _fields_ = [("tile", C.c_int32), ("cluster", C.c_int32), ("threads", C.c_int32), ("device", C.c_int32)]
 
 
+PROPAG_STATIC_MAX_CELLS = 1 << 20  # propag_run_device_static's fixed scratch
+
 STAT_FIELDS = ("rounds", "launches", "sweeps", "evaluations", "improvements", "dda_steps",
                "refbox_scans", "burned", "gathers", "cyc_first", "cyc_eval", "cyc_commit",
                "cyc_stage")
@@ -159,6 +161,7 @@ SIGNATURES = {
     "propag_engine_run": (C.c_int, [C.c_void_p, C.POINTER(PropagJob), C.c_uint32, C.c_void_p,
                                     C.POINTER(PropagStats)]),
     "propag_engine_last_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float * 3)]),
+    "propag_run_device_static": (C.c_int, [C.POINTER(PropagJob), C.c_void_p, C.POINTER(PropagStats)]),
     "propag_run_host": (C.c_int, [C.POINTER(Settings), C.POINTER(PropagTerrainPtrs),
                                   C.POINTER(PropagIgnition), C.c_uint64, C.POINTER(PropagOptions),
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PropagStats)]),
