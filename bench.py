@@ -2,11 +2,16 @@
 """Benchmark of the wildfire hot path (fire behaviour + arrival-time
 propagation) on B200.
 
-Default workload: the large heterogeneous single scenario (4096 x 4096 cells
-at 5 m, ridged terrain up to 45 deg, 12 % non-burnable lakes and roads,
-smooth random wind 0-15 m/s, per-cell moisture jitter, 20 ignitions,
+Headline workload: the large heterogeneous single scenario (4096 x 4096
+cells at 5 m, ridged terrain up to 45 deg, 12 % non-burnable lakes and
+roads, smooth random wind 0-15 m/s, per-cell moisture jitter, 20 ignitions,
 max_time 43200 s), seeded synthetic inputs.  A step = fire behaviour over
 every cell + boundaries + propagation + post mask for that scenario.
+
+Batched leg (``batched`` in the JSON line): the 256-member ensemble on a
+shared 1024 x 1024 terrain (per-member wind, dead moisture and ignition,
+max_time 21600 s); all members in one persistent launch against the same
+members run one by one through the plain path, with per-scenario latency.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
   python bench.py --impl reference ...   # the CPU implementation of the path
@@ -41,6 +46,12 @@ UNIT = "scenarios/s"
 FIRE_BYTES_PER_CELL = 49  # 37 B in (u8 fuel + 9 f32) + 12 B out (3 f32)
 # propagation: 20 B per cell evaluation + 8 B per improvement + 4 B per
 # reference-time gather (algorithmic, neighbours reused on chip)
+
+# Propagation work of the full workloads (cell evaluations), as counted on the
+# device by the engine and identically by the CPU restatement (same schedule,
+# bit-identical results).  The CPU legs time a bounded crop and scale by it;
+# the GPU leg reports whether its own count still agrees.
+WORK_EVALUATIONS = {"config1": 264198198}
 
 
 def _peaks():
@@ -121,22 +132,28 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def cpu_baseline(sc, evaluations_full: int, threads: int, budget_s: float = 20.0) -> dict:
-    """Times the CPU restatement (oracle) on a bounded crop of the workload and
-    scales by the propagation work (cell evaluations) of the full scenario."""
+def cpu_baseline(sc, evaluations_full: int, threads: int, budget_s: float = 20.0,
+                 use_firelib_c: bool = False) -> dict:
+    """Times the CPU path on a bounded sample of the workload: fire behaviour
+    on 1/16 of the cells (the reference's fireLib.c when asked and built,
+    else the FP64 restatement), propagation by the CPU restatement on a crop
+    around the first ignition, scaled by the full scenario's cell
+    evaluations."""
     from oracle import oracle as O
     t0 = time.perf_counter()
     ncell = sc.width * sc.height
-    # fire behaviour: FP64 restatement over a 1/16 sample of the cells
     k = max(1, ncell // 16)
     samp = {kk: np.ascontiguousarray(v.ravel()[:k]) for kk, v in sc.terrain.items()}
+    fire_kind = "fireLib.c (reference, 1 thread)" if use_firelib_c and O.have_firelib_c() else \
+        "FP64 restatement (1 thread)"
     tf = time.perf_counter()
-    O.burn_f64(samp)
+    if fire_kind.startswith("fireLib.c"):
+        O.burn_firelib_c(samp)
+    else:
+        O.burn_f64(samp)
     fire_s = (time.perf_counter() - tf) * (ncell / k)
-    # propagation: crop around the first ignition, growing until the budget
     crop = 256
     cx, cy = sc.ignitions[0][0], sc.ignitions[0][1]
-    prop_rate = None
     while True:
         x0 = int(min(max(cx - crop // 2, 0), sc.width - crop))
         y0 = int(min(max(cy - crop // 2, 0), sc.height - crop))
@@ -154,26 +171,33 @@ def cpu_baseline(sc, evaluations_full: int, threads: int, budget_s: float = 20.0
             break
         crop *= 2
     prop_s = evaluations_full / prop_rate
-    return {"value": 1.0 / (fire_s + prop_s), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"CPU restatement (oracle/): FP64 fire behaviour on {k} cells scaled to "
-                       f"{ncell}; propagation on a {crop}x{crop} crop around the first ignition "
-                       f"({prop_rate:.3g} cell evaluations/s on {threads} threads) scaled to the "
-                       f"full scenario's {evaluations_full} evaluations"),
+    return {"value": 1.0 / (fire_s + prop_s), "unit": UNIT, "cores": threads,
+            # the propagation (over 95 % of the time) is always the CPU restatement
+            "kind": "port",
+            "sample": (f"fire behaviour: {fire_kind} on {k} of {ncell} cells, scaled; propagation: "
+                       f"CPU restatement of propag.cu (the reference has no CPU propagation) on a "
+                       f"{crop}x{crop} crop around the first ignition, {prop_rate:.3g} cell "
+                       f"evaluations/s on {threads} threads, scaled to the full scenario's "
+                       f"{evaluations_full} evaluations"),
             "fire_s": fire_s, "propagation_s": prop_s}
 
 
 def run_reference(args):
+    """The reference's CPU implementation of the path on this host's cores:
+    its own fireLib.c for fire behaviour when it was built here (oracle/_ref),
+    and the CPU restatement of its propagation kernel."""
     rank, world, _ = _rank_env()
     if rank != 0:
         return
     sc, desc = _workload(args.workload)
     threads = os.cpu_count() or 1
-    # the full scenario's propagation work, measured on B200 with the same
-    # schedule (bit-identical evaluations on both sides)
-    evals = {"config1": 1.0e9}.get(args.workload)
+    evals = WORK_EVALUATIONS.get(args.workload)
+    if evals is None:
+        raise SystemExit(f"no recorded propagation work for workload {args.workload}")
     vals = []
+    cb = None
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(sc, int(evals or 0) or 10_000_000, threads, budget_s=10.0)
+        cb = cpu_baseline(sc, evals, threads, budget_s=10.0, use_firelib_c=True)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = float(np.median(vals))
@@ -183,6 +207,115 @@ def run_reference(args):
             "cpu_baseline": dict(cb, value=v),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def ensemble_leg(lib, L, dev, stream, n_members: int, steps: int, warmup: int,
+                 plain_members: int) -> dict:
+    """The 256-member ensemble on a shared 1024 x 1024 terrain: every member's
+    fire pass plus ONE persistent engine launch for all members, against the
+    plain path (fire + a one-job engine run per member, one after another)."""
+    import torch
+    from py_propag import scenarios as S
+    base, members = S.config2(n=n_members)
+    N = base.width * base.height
+    words = (N + 31) // 32
+    sptr = C.c_void_p(stream.cuda_stream)
+    bt = {k: torch.from_numpy(np.ascontiguousarray(v).ravel()).to(dev) for k, v in base.terrain.items()}
+    jobs, keep = [], []
+    for m in members:
+        t = dict(bt)
+        t["wind_speed"] = torch.full((N,), m["wind_speed"], dtype=torch.float32, device=dev)
+        t["wind_azimuth"] = torch.full((N,), m["wind_azimuth"], dtype=torch.float32, device=dev)
+        for k in ("d1hr", "d10hr", "d100hr"):
+            t[k] = bt[k] + np.float32(m["dead_offset"])
+        ptrs = L.PropagTerrainPtrs(*[t[k].data_ptr() for k in L.TERRAIN_FIELDS])
+        fire = [torch.empty(N, dtype=torch.float32, device=dev) for _ in range(3)]
+        ign = np.array([m["ignition"]], dtype=[("x", "<u4"), ("y", "<u4"), ("t", "<f4")])
+        ign_d = torch.from_numpy(np.frombuffer(ign.tobytes(), np.uint8).copy()).to(dev)
+        out = torch.empty(N, dtype=torch.float32, device=dev)
+        rx = torch.empty(N, dtype=torch.int16, device=dev)
+        ry = torch.empty(N, dtype=torch.int16, device=dev)
+        bnd = torch.empty(words, dtype=torch.int32, device=dev)
+        j = L.PropagJob()
+        j.width, j.height, j.dx, j.dy = base.width, base.height, base.dx, base.dy
+        j.max_time, j.tile = m["max_time"], 0
+        j.speed_max, j.azimuth_max, j.eccentricity = (f.data_ptr() for f in fire)
+        j.ignitions, j.n_ignitions = ign_d.data_ptr(), 1
+        j.time, j.refs_x, j.refs_y, j.boundaries = out.data_ptr(), rx.data_ptr(), ry.data_ptr(), bnd.data_ptr()
+        jobs.append(j)
+        keep.append((t, ptrs, fire, ign_d, out, rx, ry, bnd))
+    arr = (L.PropagJob * len(jobs))(*jobs)
+    eng = lib.propag_engine_create(C.byref(L.PropagOptions(0, 0, 0, -1)))
+    if not eng:
+        raise RuntimeError(L.last_error())
+
+    def fire(i):
+        f = keep[i][2]
+        if lib.propag_fire_simple_device(N, C.byref(keep[i][1]), f[0].data_ptr(), f[1].data_ptr(),
+                                         f[2].data_ptr(), sptr):
+            raise RuntimeError(L.last_error())
+
+    def run(first, count, stats=None):
+        p = C.cast(C.addressof(arr) + first * C.sizeof(L.PropagJob), C.POINTER(L.PropagJob))
+        if lib.propag_engine_run(eng, p, count, sptr, stats):
+            raise RuntimeError(L.last_error())
+
+    def batched_step(stats=None):
+        for i in range(len(jobs)):
+            fire(i)
+        run(0, len(jobs), stats)
+
+    # plain path: each member alone, in order (its own latency is its time)
+    plain_members = min(plain_members, len(jobs))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fire(0)
+    run(0, 1)
+    torch.cuda.synchronize()
+    plain_ms, plain_out = [], []
+    for i in range(plain_members):
+        e0.record(stream)
+        fire(i)
+        run(i, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms.append(e0.elapsed_time(e1))
+        plain_out.append(keep[i][4].clone())
+    # batched: all members in one launch
+    st = (L.PropagStats * len(jobs))()
+    batched_step(st)  # first run: statistics and per-member device timestamps
+    for _ in range(warmup):
+        batched_step()
+    torch.cuda.synchronize()
+    step_ms = []
+    for _ in range(steps):
+        e0.record(stream)
+        batched_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    same = all(torch.equal(plain_out[i], keep[i][4]) for i in range(plain_members))
+    t0 = min(s.t_start_ns for s in st)
+    fire_prep_ms = float(np.median(step_ms)) - (max(s.t_done_ns for s in st) - t0) / 1e6
+    lat = np.array([(s.t_done_ns - t0) / 1e6 + max(fire_prep_ms, 0.0) for s in st])
+    lib.propag_engine_destroy(eng)
+    batched = len(jobs) / (float(np.median(step_ms)) / 1e3)
+    plain = len(plain_ms) / (float(np.sum(plain_ms)) / 1e3)
+    return {
+        "workload": f"config2: {len(jobs)}-member ensemble on a shared {base.width}x{base.height} "
+                    f"terrain, per-member wind/moisture/ignition, max_time 21600 s",
+        "value": batched, "unit": UNIT, "ms_per_batch": float(np.median(step_ms)),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "note": "batch start to each member's propagation end (device clock), "
+                               "plus the batch's fire/prep time"},
+        "plain": {"value": plain, "unit": UNIT, "members_timed": len(plain_ms),
+                  "latency_ms": {"p50": float(np.percentile(plain_ms, 50)),
+                                 "p99": float(np.percentile(plain_ms, 99))}},
+        "speedup_vs_plain": batched / plain,
+        "matches_plain_bitwise": bool(same),
+        "gpu_launches_per_batch": len(jobs) + 4,
+        "sweeps_mean": float(np.mean([s.sweeps for s in st])),
+        "evaluations": int(sum(s.evaluations for s in st)),
+    }
 
 
 def main():
@@ -195,10 +328,19 @@ def main():
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cluster", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ensemble", type=int, default=256, help="members of the batched leg (0 = skip)")
+    ap.add_argument("--plain-members", type=int, default=256,
+                    help="ensemble members timed one by one on the plain path")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.warmup < 0 or args.steps < 1:
+        raise SystemExit("--steps >= 1 and --warmup >= 0")
+    bench_b200(args)
 
+
+def bench_b200(args):
     import torch
     import torch.distributed as dist
 
@@ -234,20 +376,20 @@ def main():
     job.ignitions, job.n_ignitions = ign_dev.data_ptr(), len(sc.ignitions)
     job.time, job.refs_x, job.refs_y, job.boundaries = (time_d.data_ptr(), rx_d.data_ptr(),
                                                         ry_d.data_ptr(), bnd_d.data_ptr())
-    opt = L.PropagOptions(args.tile, args.cluster, 0, -1)
-    eng = lib.propag_engine_create(C.byref(opt))
+    eng = lib.propag_engine_create(C.byref(L.PropagOptions(args.tile, args.cluster, 0, -1)))
     if not eng:
         raise RuntimeError(L.last_error())
     stream = torch.cuda.current_stream(dev)
     sptr = C.c_void_p(stream.cuda_stream)
 
-    def step(stats=None):
-        rc = lib.propag_fire_simple_device(N, C.byref(ptrs), fire[0].data_ptr(), fire[1].data_ptr(),
-                                           fire[2].data_ptr(), sptr)
-        if rc:
+    def fire_pass():
+        if lib.propag_fire_simple_device(N, C.byref(ptrs), fire[0].data_ptr(), fire[1].data_ptr(),
+                                         fire[2].data_ptr(), sptr):
             raise RuntimeError(L.last_error())
-        rc = lib.propag_engine_run(eng, C.byref(job), 1, sptr, stats)
-        if rc:
+
+    def step(stats=None):
+        fire_pass()
+        if lib.propag_engine_run(eng, C.byref(job), 1, sptr, stats):
             raise RuntimeError(L.last_error())
 
     st = L.PropagStats()
@@ -272,13 +414,11 @@ def main():
     for i in range(args.steps):
         ev_step[i][0].record(stream)
         ev_fire[i][0].record(stream)
-        rc = lib.propag_fire_simple_device(N, C.byref(ptrs), fire[0].data_ptr(), fire[1].data_ptr(),
-                                           fire[2].data_ptr(), sptr)
+        fire_pass()
         ev_fire[i][1].record(stream)
-        rc |= lib.propag_engine_run(eng, C.byref(job), 1, sptr, None)
-        ev_step[i][1].record(stream)
-        if rc:
+        if lib.propag_engine_run(eng, C.byref(job), 1, sptr, None):
             raise RuntimeError(L.last_error())
+        ev_step[i][1].record(stream)
         ms = (C.c_float * 3)()
         lib.propag_engine_last_times(eng, ms)  # waits for this step
         eng_ms.append(list(ms))
@@ -294,8 +434,64 @@ def main():
     fire_ms = [a.elapsed_time(b) for a, b in ev_fire]
     prop_ms = [m[1] for m in eng_ms]
     value = world * args.steps / (total_ms / 1e3)
+    dev_time = time_d.cpu().numpy()
 
-    # end to end through the C-ABI host entry point (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_leg(lib, L, pp, sc, args, world, dev, dev_time)
+
+    peak, peak_kind = _peaks()
+    prop_bytes = 20 * stats["evaluations"] + 8 * stats["improvements"] + 4 * stats["gathers"]
+    prop_s = float(np.mean(prop_ms)) / 1e3
+    fire_s = float(np.mean(fire_ms)) / 1e3
+    ach = prop_bytes / prop_s / 1e9
+    fire_ach = FIRE_BYTES_PER_CELL * N / fire_s / 1e9
+    known = WORK_EVALUATIONS.get(args.workload)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "cells": N, "tile": args.tile or 323, "cluster": args.cluster,
+                   "l2": "inputs larger than L2 (terrain 37 B/cell, 620 MB at 4096^2)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                       "fire_kernel": float(np.mean(fire_ms)), "propagation_kernel": float(np.mean(prop_ms)),
+                       "prep": float(np.mean([m[0] for m in eng_ms])),
+                       "post": float(np.mean([m[2] for m in eng_ms]))},
+        "cells_per_s": N * world * args.steps / (total_ms / 1e3),
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "kernel": "engine_kernel (propagation)", "achieved": ach,
+                     "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": None,
+                     "algorithmic_bytes": prop_bytes, "peak_source": peak_kind},
+        "kernels": {"fire_kernel": {"achieved": fire_ach, "peak": peak, "unit": "GB/s",
+                                    "frac": fire_ach / peak, "bytes": FIRE_BYTES_PER_CELL * N}},
+        "workload_stats": stats,
+        "work_matches_recorded": (stats["evaluations"] == known) if known else None,
+        "gpu_launches": 5 * args.steps,
+        "clocks": clk,
+    }
+    lib.propag_engine_destroy(eng)
+    del t_dev, fire, time_d, rx_d, ry_d, bnd_d
+    if args.ensemble > 0:
+        line["batched"] = ensemble_leg(lib, L, dev, stream, args.ensemble, args.steps, args.warmup,
+                                       args.plain_members)
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(sc, stats["evaluations"], os.cpu_count() or 1)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def e2e_leg(lib, L, pp, sc, args, world, dev, dev_time):
+    """The same metric through the C-ABI host entry point (propag_run_host):
+    pinned host inputs copied in and results copied out inside the timed
+    region, every step."""
+    import torch
+    import torch.distributed as dist
+    N = sc.width * sc.height
+    words = (N + 31) // 32
     pin = {k: torch.from_numpy(np.ascontiguousarray(v).ravel()).pin_memory() for k, v in sc.terrain.items()}
     hptrs = L.PropagTerrainPtrs(*[pin[k].data_ptr() for k in L.TERRAIN_FIELDS])
     out_t = torch.empty(N, dtype=torch.float32).pin_memory()
@@ -309,10 +505,9 @@ def main():
     hopt = L.PropagOptions(args.tile, args.cluster, 0, -1)
 
     def e2e_step():
-        rc = lib.propag_run_host(C.byref(settings), C.byref(hptrs), ign_arr, len(sc.ignitions),
-                                 C.byref(hopt), out_t.data_ptr(), out_rx.data_ptr(), out_ry.data_ptr(),
-                                 out_b.data_ptr(), None)
-        if rc:
+        if lib.propag_run_host(C.byref(settings), C.byref(hptrs), ign_arr, len(sc.ignitions),
+                               C.byref(hopt), out_t.data_ptr(), out_rx.data_ptr(), out_ry.data_ptr(),
+                               out_b.data_ptr(), None):
             raise RuntimeError(L.last_error())
 
     for _ in range(max(1, args.warmup)):
@@ -327,47 +522,12 @@ def main():
         tt = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
-    same = np.array_equal(out_t.numpy().view(np.uint32), time_d.cpu().numpy().view(np.uint32))
-    h2d = N * 37 + len(sc.ignitions) * 12
-    d2h = N * 4 + N * 4 + words * 4
-
-    peak, peak_kind = _peaks()
-    prop_bytes = 20 * stats["evaluations"] + 8 * stats["improvements"] + 4 * stats["gathers"]
-    prop_s = float(np.mean(prop_ms)) / 1e3
-    fire_s = float(np.mean(fire_ms)) / 1e3
-    ach = prop_bytes / prop_s / 1e9
-    fire_ach = FIRE_BYTES_PER_CELL * N / fire_s / 1e9
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": desc, "cells": N, "tile": args.tile or 323, "cluster": args.cluster,
-                   "l2": "inputs larger than L2 (620 MB terrain, 16.8M-cell state)",
-                   "parallelism": "replicas" if world > 1 else "single"},
-        "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
-                       "fire_kernel": float(np.mean(fire_ms)), "propagation_kernel": float(np.mean(prop_ms)),
-                       "prep": float(np.mean([m[0] for m in eng_ms])),
-                       "post": float(np.mean([m[2] for m in eng_ms]))},
-        "cells_per_s": N * world * args.steps / (total_ms / 1e3),
-        "e2e": {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "matches_device_path": bool(same)},
-        "roofline": {"bound": "hbm", "kernel": "propagation engine", "achieved": ach, "peak": peak,
-                     "unit": "GB/s", "frac": ach / peak, "traffic": None,
-                     "algorithmic_bytes": prop_bytes, "peak_source": peak_kind},
-        "kernels": {"fire_behaviour": {"achieved": fire_ach, "peak": peak, "unit": "GB/s",
-                                       "frac": fire_ach / peak, "bytes": FIRE_BYTES_PER_CELL * N}},
-        "workload_stats": stats,
-        "gpu_launches": 5 * args.steps,
-        "clocks": clk,
-    }
-    if rank == 0 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(sc, stats["evaluations"], os.cpu_count() or 1)
-    lib.propag_engine_destroy(eng)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    same = np.array_equal(out_t.numpy().view(np.uint32), dev_time.view(np.uint32))
+    return {"value": world * args.steps / e2e_s, "unit": UNIT,
+            "h2d_bytes_per_step": N * 37 + len(sc.ignitions) * 12,
+            "d2h_bytes_per_step": N * 4 + N * 4 + words * 4, "matches_device_path": bool(same),
+            "note": "propag_run_host: pinned host terrain in, times/refs/boundaries out, "
+                    "fire + propagation on the device, wall clock"}
 
 
 if __name__ == "__main__":

@@ -128,6 +128,8 @@ typedef struct PropagStats {
   uint64_t cyc_first, cyc_eval, cyc_commit, cyc_stage;
   uint32_t status;       /* 0 ok; nonzero: device-side error code */
   uint32_t max_walk;     /* longest line-of-sight walk (cells) */
+  uint64_t t_start_ns;   /* device clock (ns) when a cluster took the job */
+  uint64_t t_done_ns;    /* device clock (ns) when its propagation finished */
 } PropagStats;
 
 /* One scenario of a batch.  All pointers are device pointers; time, refs and

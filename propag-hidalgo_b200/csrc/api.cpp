@@ -377,6 +377,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
       o.cyc_stage = hs[i].cyc_stage;
       o.status = hs[i].status;
       o.max_walk = hs[i].max_walk;
+      o.t_start_ns = hs[i].t_start_ns;
+      o.t_done_ns = hs[i].t_done_ns;
     }
     for (uint32_t i = 0; i < n_jobs; ++i)
       if (hs[i].status) return fail(PROPAG_ERR_TIMEOUT, "job " + std::to_string(i) + ": sweep limit reached");
@@ -515,6 +517,8 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
     o.cyc_stage = h.cyc_stage;
     o.status = h.status;
     o.max_walk = h.max_walk;
+    o.t_start_ns = h.t_start_ns;
+    o.t_done_ns = h.t_done_ns;
     if (h.status) return fail(PROPAG_ERR_TIMEOUT, "sweep limit reached");
   }
   return PROPAG_OK;

@@ -53,6 +53,13 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kEngineThreads = 512;
 constexpr uint32_t kEmptyBox = 0xFFFFFFFFu;
 
+// The GPU's global nanosecond clock (comparable across SMs and launches).
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // ---------------------------------------------------------------- prep ----
 // Boundary bits (find_boundaries) packed with a warp ballot, plus the initial
 // state: time = FLT_MAX, no reference, empty referrer boxes.
@@ -854,6 +861,7 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
     __syncthreads();
     const JobDev &j = js;  // shared-memory copy: frees registers
     StatsDev *st = stats + jid;
+    if (tid == 0) st->t_start_ns = globaltimer_ns();
     SweepCtx cx;
     cx.leader = tid == 0;
     cx.max_sweeps = max_sweeps;
@@ -902,6 +910,7 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
       st->cyc_commit = cx.cyc[2];
       st->cyc_stage = cx.cyc[3];
       if (cx.abort) st->status = kStatusSweepLimit;
+      st->t_done_ns = globaltimer_ns();
     }
     sync_cluster();
   }

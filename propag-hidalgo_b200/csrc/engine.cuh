@@ -52,6 +52,9 @@ struct StatsDev {
   // included): first sweeps of tile launches, evaluate, commit, staging
   unsigned long long cyc_first, cyc_eval, cyc_commit, cyc_stage;
   uint32_t status, max_walk;
+  // device clock (%globaltimer, ns) when a cluster took the job and when its
+  // propagation finished
+  unsigned long long t_start_ns, t_done_ns;
 };
 
 constexpr uint32_t kStatusSweepLimit = 1;

@@ -115,10 +115,12 @@ STAT_FIELDS = ("rounds", "launches", "sweeps", "evaluations", "improvements", "d
 
 class PropagStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in STAT_FIELDS] + [("status", C.c_uint32),
-                                                         ("max_walk", C.c_uint32)]
+                                                         ("max_walk", C.c_uint32),
+                                                         ("t_start_ns", C.c_uint64),
+                                                         ("t_done_ns", C.c_uint64)]
 
     def as_dict(self):
-        return {k: int(getattr(self, k)) for k in STAT_FIELDS + ("status", "max_walk")}
+        return {k: int(getattr(self, k)) for k in STAT_FIELDS + ("status", "max_walk", "t_start_ns", "t_done_ns")}
 
 
 class PropagJob(C.Structure):
