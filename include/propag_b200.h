@@ -178,7 +178,7 @@ int propag_engine_last_times(propag_engine *engine, float ms[3]);
  *
  * Same kernels, schedule and results as propag_engine_run with one job, but
  * its scratch (references, referrer boxes, boundary bits, job descriptor,
- * counters, statistics) lives in one fixed device array of about 20.1 MiB,
+ * counters, statistics, list overflow) lives in one fixed device array of about 25 MiB,
  * reserved by the CUDA driver when the library's module holding it is loaded.
  * The call makes no cudaMalloc, cudaFree or cudaMallocHost, creates no events
  * and uses no caching allocator.  It is meant for callers that cannot

@@ -267,13 +267,27 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   auto fits = [&](uint32_t i, int c) { return smem_bytes(tw[i], th[i], c) <= budget; };
   int csize = e->csize;
   if (csize == 0) {
-    // the smallest cluster that holds every job's tile (more clusters, more
-    // scenarios at once); when some tile never fits, as many clusters as
-    // there are jobs, as large as the machine allows
-    for (int c = 1; c <= 16 && csize == 0; c *= 2) {
+    // among the cluster sizes that hold every job's tile, the one that runs
+    // the most jobs at once (resident clusters, up to the job count); ties go
+    // to the larger cluster, which finishes each job sooner.  When some tile
+    // never fits, as many clusters as there are jobs, as large as the
+    // machine allows.
+    uint32_t best_conc = 0;
+    for (int c = 16; c >= 1; c /= 2) {
       bool all = true;
-      for (uint32_t i = 0; i < n_jobs && all; ++i) all = fits(i, c);
-      if (all) csize = c;
+      size_t need = 0;
+      for (uint32_t i = 0; i < n_jobs && all; ++i) {
+        all = fits(i, c);
+        need = std::max(need, smem_bytes(tw[i], th[i], c));
+      }
+      if (!all) continue;
+      int mc = 0;
+      CK(engine_max_clusters(c, e->threads, need, &mc));
+      const uint32_t conc = std::min<uint32_t>(n_jobs, (uint32_t)std::max(mc, 0));
+      if (conc > best_conc) {
+        best_conc = conc;
+        csize = c;
+      }
     }
     if (csize == 0) {
       int ctas = 0;
@@ -282,13 +296,17 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
       while (csize < 16 && (uint64_t)(csize * 2) * n_jobs <= (uint64_t)std::max(ctas, 1)) csize *= 2;
     }
   }
-  size_t smem = 0, tn_max = 1;
+  size_t smem = 0, tn_max = 1, ovf_cap = 0;
   for (uint32_t i = 0; i < n_jobs; ++i) {
-    jd[i].smem_tile = fits(i, csize) ? 1 : 0;
-    if (jd[i].smem_tile)
-      smem = std::max(smem, smem_bytes(tw[i], th[i], csize));
-    else
+    // exact referrer boxes when they fit, else the coarse ones
+    const bool exact = smem_bytes(tw[i], th[i], csize, true) <= budget;
+    jd[i].smem_tile = exact ? kSmemTileExact : fits(i, csize) ? kSmemTileCoarse : kSmemTileGlobal;
+    if (jd[i].smem_tile != kSmemTileGlobal) {
+      smem = std::max(smem, smem_bytes(tw[i], th[i], csize, exact));
+      ovf_cap = std::max<size_t>(ovf_cap, (size_t)smem_cap(tw[i], th[i], csize));
+    } else {
       tn_max = std::max<size_t>(tn_max, (size_t)tw[i] * (size_t)th[i]);
+    }
   }
   int max_clusters = 0;
   CK(engine_max_clusters(csize, e->threads, smem, &max_clusters));
@@ -297,8 +315,11 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   e->last_cluster = csize;
   e->last_smem = smem;
   const size_t words_max = tn_max / 32 + 1;
+  const size_t ovf_list_bytes = align_up((size_t)csize * ovf_cap * 2, 256);
+  const size_t ovf_upd_bytes = align_up((size_t)csize * ovf_cap * sizeof(Update), 256);
   const size_t slot_bytes = align_up(tn_max * 4, 256) * 3 + align_up(words_max * 4, 256) +
-                            align_up(tn_max * sizeof(Update), 256) + 256;
+                            align_up(tn_max * sizeof(Update), 256) + 256 + ovf_list_bytes +
+                            ovf_upd_bytes;
   CK(e->slot_scratch.reserve(slot_bytes * n_slots, stream));
   // meta: jobs, slots, stats, queue
   const size_t meta_jobs = align_up(sizeof(JobDev) * n_jobs, 256);
@@ -332,6 +353,12 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     sd.upd = e->slot_scratch.at<Update>(o);
     o += align_up(tn_max * sizeof(Update), 256);
     sd.ctr = e->slot_scratch.at<uint32_t>(o);
+    o += 256;
+    sd.ovf_list = e->slot_scratch.at<uint16_t>(o);
+    o += ovf_list_bytes;
+    sd.ovf_upd = e->slot_scratch.at<Update>(o);
+    sd.ovf_cap = (uint32_t)ovf_cap;
+    sd.pad = 0;
     // the dirty bitmap and counters must start cleared
     CK(cudaMemsetAsync(sd.dirty, 0, words_max * 4, stream));
     CK(cudaMemsetAsync(sd.ctr, 0, 64, stream));
@@ -432,17 +459,17 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   int T = j.tile ? j.tile : PROPAG_DEFAULT_TILE;
   if (T == PROPAG_TILE_WHOLE_GRID || T <= 0) T = (int)std::max(j.width, j.height);
   const int tw = std::min<int>(T, (int)j.width), th = std::min<int>(T, (int)j.height);
-  // the smallest cluster whose shared memory holds the tile and its halo
+  // one job: the largest cluster (16 CTAs), which finishes it soonest
   const size_t budget = 200 * 1024;
-  int csize = 0;
-  for (int c = 1; c <= 16 && csize == 0; c *= 2)
-    if (smem_bytes(tw, th, c) <= budget) csize = c;
-  if (csize == 0)
+  const int csize = 16;
+  if (smem_bytes(tw, th, csize) > budget ||
+      (size_t)csize * (size_t)smem_cap(tw, th, csize) > kStaticOvfSlots)
     return fail(PROPAG_ERR_INVALID,
                 "propag_run_device_static: a " + std::to_string(tw) + " x " + std::to_string(th) +
                     " tile does not fit in a 16-CTA cluster's shared memory (use a tile side <= 323 or "
                     "propag_engine_run)");
-  const size_t smem = smem_bytes(tw, th, csize);
+  const bool exact = smem_bytes(tw, th, csize, true) <= budget;
+  const size_t smem = smem_bytes(tw, th, csize, exact);
   int dev = 0;
   CK(cudaGetDevice(&dev));
   char *base = nullptr;
@@ -468,7 +495,7 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   d.TX = (int)((j.width + T - 1) / T);
   d.TY = (int)((j.height + T - 1) / T);
   d.north_up = j.dy < 0 ? 1 : 0;
-  d.smem_tile = 1;
+  d.smem_tile = exact ? kSmemTileExact : kSmemTileCoarse;
   d.speed = j.speed_max;
   d.az = j.azimuth_max;
   d.ecc = j.eccentricity;
@@ -485,8 +512,11 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   d.box_x1 = cells + 3 * kStaticMaxCells;
   d.box_y1 = cells + 4 * kStaticMaxCells;
   d.bnd = j.boundaries ? j.boundaries : reinterpret_cast<uint32_t *>(base + kStaticBndOff);
-  SlotDev s{};  // shared-memory tiles use only the counters
+  SlotDev s{};  // shared-memory tiles use the counters and the list overflow
   s.ctr = reinterpret_cast<uint32_t *>(base + kStaticCtrOff);
+  s.ovf_list = reinterpret_cast<uint16_t *>(base + kStaticOvfListOff);
+  s.ovf_upd = reinterpret_cast<Update *>(base + kStaticOvfUpdOff);
+  s.ovf_cap = (uint32_t)smem_cap(tw, th, csize);
   JobDev *d_job = reinterpret_cast<JobDev *>(base + kStaticJobOff);
   SlotDev *d_slot = reinterpret_cast<SlotDev *>(base + kStaticSlotOff);
   StatsDev *d_stats = reinterpret_cast<StatsDev *>(base + kStaticStatsOff);

@@ -524,53 +524,149 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
 struct SmemTile {
   float *time;
   uint32_t *ref;
-  uint32_t *blo, *bhi;  // referrer box corners, x | y << 16 (blo 0xFFFFFFFF = empty)
-  float *utime;         // pending updates: time, reference, local slot
+  // referrer box of each slot restricted to the staged region, in the job's
+  // codec (BoxCoarse or BoxExact); the codec's kEmpty when no referrer lies
+  // inside
+  void *box;
+  uint16_t *list;   // this sweep's cells to evaluate (local slot index); kSmemListCap
+  uint16_t *uidx;   // pending updates: local slot, time, reference; kSmemUpdCap
+  float *utime;
   uint32_t *uref;
-  uint16_t *list;       // this sweep's cells to evaluate (local slot index)
-  uint16_t *uidx;
-  uint32_t *dirty;      // bit per local slot: evaluate in the next sweep
-  uint32_t *ctr;        // [0] list size, [1] local updates, [2..3] cluster updates (parity)
+  uint32_t *dirty;  // bit per local slot: evaluate in the next sweep
+  uint32_t *grown;  // bit per local slot: a referrer joined its staged box in this launch
+  uint32_t *ctr;    // [0] list size, [1] local updates, [2..3] cluster updates (parity)
+  uint16_t *ovf_list;  // this CTA's global overflow of list / updates
+  Update *ovf_upd;
 };
 
-__device__ __forceinline__ SmemTile carve_smem(char *base, int cap) {
+__device__ __forceinline__ SmemTile carve_smem(char *base, int cap, int box_bytes, const SlotDev &s,
+                                              int rank) {
   SmemTile t;
+  t.box = base;  // first: 8-byte aligned for BoxExact
+  base += (size_t)cap * box_bytes;
   t.time = (float *)base;
   base += (size_t)cap * 4;
   t.ref = (uint32_t *)base;
   base += (size_t)cap * 4;
-  t.blo = (uint32_t *)base;
-  base += (size_t)cap * 4;
-  t.bhi = (uint32_t *)base;
-  base += (size_t)cap * 4;
   t.utime = (float *)base;
-  base += (size_t)cap * 4;
+  base += (size_t)kSmemUpdCap * 4;
   t.uref = (uint32_t *)base;
-  base += (size_t)cap * 4;
+  base += (size_t)kSmemUpdCap * 4;
   t.list = (uint16_t *)base;
-  base += (size_t)cap * 2;
+  base += (size_t)kSmemListCap * 2;
   t.uidx = (uint16_t *)base;
-  base += (size_t)cap * 2;
+  base += (size_t)kSmemUpdCap * 2;
   t.dirty = (uint32_t *)(((uintptr_t)base + 3) & ~(uintptr_t)3);
   base = (char *)(t.dirty + (cap / 32 + 1));
+  t.grown = (uint32_t *)base;
+  base = (char *)(t.grown + (cap / 32 + 1));
   t.ctr = (uint32_t *)(((uintptr_t)base + 15) & ~(uintptr_t)15);
+  t.ovf_list = s.ovf_list + (size_t)rank * s.ovf_cap;
+  t.ovf_upd = s.ovf_upd + (size_t)rank * s.ovf_cap;
   return t;
 }
 
+// Work-list and update-list entries: shared memory first, then the overflow.
+__device__ __forceinline__ void list_put(const SmemTile &t, uint32_t i, uint32_t slot) {
+  if (i < (uint32_t)kSmemListCap)
+    t.list[i] = (uint16_t)slot;
+  else
+    t.ovf_list[i - kSmemListCap] = (uint16_t)slot;
+}
+__device__ __forceinline__ uint32_t list_get(const SmemTile &t, uint32_t i) {
+  return i < (uint32_t)kSmemListCap ? t.list[i] : __ldcg(t.ovf_list + (i - kSmemListCap));
+}
+__device__ __forceinline__ void upd_put(const SmemTile &t, uint32_t i, uint32_t slot, float time,
+                                        uint32_t ref) {
+  if (i < (uint32_t)kSmemUpdCap) {
+    t.uidx[i] = (uint16_t)slot;
+    t.utime[i] = time;
+    t.uref[i] = ref;
+  } else {
+    t.ovf_upd[i - kSmemUpdCap] = Update{slot, time, ref, 0u};
+  }
+}
+__device__ __forceinline__ void upd_get(const SmemTile &t, uint32_t i, uint32_t &slot, float &time,
+                                        uint32_t &ref) {
+  if (i < (uint32_t)kSmemUpdCap) {
+    slot = t.uidx[i];
+    time = t.utime[i];
+    ref = t.uref[i];
+  } else {
+    const Update u = t.ovf_upd[i - kSmemUpdCap];
+    slot = u.k;
+    time = u.time;
+    ref = u.ref;
+  }
+}
+
+// Staged referrer-box codecs.  A box is [hx0, hx1] x [hy0, hy1] in halo-local
+// cells; grow() adds one cell with a compare-and-swap loop (per-field min of
+// the low corner, max of the high corner).
+//   BoxCoarse: one u32, a byte per corner in units of 1 << sh cells, decoded
+//              rounded outwards (4 bytes per slot; halo sides up to 510);
+//   BoxExact:  one u64, 16 bits per corner (8 bytes per slot).
+struct BoxCoarse {
+  using T = uint32_t;
+  static constexpr T kEmpty = 0x0000FFFFu;  // x0 = y0 = 255, x1 = y1 = 0
+  static __device__ __forceinline__ T pack(int hx0, int hy0, int hx1, int hy1, int sh) {
+    return (T)(hx0 >> sh) | ((T)(hy0 >> sh) << 8) | ((T)(hx1 >> sh) << 16) | ((T)(hy1 >> sh) << 24);
+  }
+  static __device__ __forceinline__ void grow(T *w, int hx, int hy, int sh) {
+    const uint32_t px = (uint32_t)(hx >> sh), py = (uint32_t)(hy >> sh);
+    const uint32_t lo = px | (py << 8) | 0xFFFF0000u;
+    const uint32_t hi = (px << 16) | (py << 24);
+    T o = *w;
+    for (;;) {
+      const T nw = (__vminu4(o, lo) & 0x0000FFFFu) | (__vmaxu4(o, hi) & 0xFFFF0000u);
+      if (nw == o) return;
+      const T pr = atomicCAS(w, o, nw);
+      if (pr == o) return;
+      o = pr;
+    }
+  }
+  static __device__ __forceinline__ void decode(T v, int sh, int &hx0, int &hy0, int &hx1, int &hy1) {
+    const int m = (1 << sh) - 1;
+    hx0 = (int)(v & 0xFFu) << sh;
+    hy0 = (int)((v >> 8) & 0xFFu) << sh;
+    hx1 = ((int)((v >> 16) & 0xFFu) << sh) + m;
+    hy1 = ((int)(v >> 24) << sh) + m;
+  }
+};
+
+struct BoxExact {
+  using T = unsigned long long;
+  static constexpr T kEmpty = 0x00000000FFFFFFFFull;  // low corner 0xFFFF, high corner 0
+  static __device__ __forceinline__ T pack(int hx0, int hy0, int hx1, int hy1, int) {
+    return (T)((uint32_t)hx0 | ((uint32_t)hy0 << 16)) | ((T)((uint32_t)hx1 | ((uint32_t)hy1 << 16)) << 32);
+  }
+  static __device__ __forceinline__ void grow(T *w, int hx, int hy, int) {
+    const uint32_t p = (uint32_t)hx | ((uint32_t)hy << 16);
+    T o = *w;
+    for (;;) {
+      const T nw = (T)__vminu2((uint32_t)o, p) | ((T)__vmaxu2((uint32_t)(o >> 32), p) << 32);
+      if (nw == o) return;
+      const T pr = atomicCAS(w, o, nw);
+      if (pr == o) return;
+      o = pr;
+    }
+  }
+  static __device__ __forceinline__ void decode(T v, int, int &hx0, int &hy0, int &hx1, int &hy1) {
+    hx0 = (int)(v & 0xFFFFu);
+    hy0 = (int)((v >> 16) & 0xFFFFu);
+    hx1 = (int)((v >> 32) & 0xFFFFu);
+    hy1 = (int)(v >> 48);
+  }
+};
+
 struct SmemGeom {
   int x0, y0, TW, TH, P, HR, C, rank, rows_mine;
+  int sh;  // box_shift: 0 when the halo side fits a byte, else 1
 };
 
 template <typename T>
 __device__ __forceinline__ T *rank_ptr(T *local, int r) {
   return cg::this_cluster().map_shared_rank(local, (unsigned)r);
-}
-
-__device__ __forceinline__ uint32_t box_pack_min(uint32_t old, int x, int y) {
-  return min(old & 0xFFFFu, (uint32_t)x) | (min(old >> 16, (uint32_t)y) << 16);
-}
-__device__ __forceinline__ uint32_t box_pack_max(uint32_t old, int x, int y) {
-  return max(old & 0xFFFFu, (uint32_t)x) | (max(old >> 16, (uint32_t)y) << 16);
 }
 
 // Marks the tile cells of the 3x3 neighbourhood of halo cell (hx, hy) in
@@ -621,20 +717,12 @@ struct SmemAcc {
   __device__ __forceinline__ float time_of(uint32_t r) const { return smem_time_of(j, sm, g, r); }
 };
 
-__device__ __forceinline__ void smem_box_cas(uint32_t *w, int x, int y, bool is_min) {
-  uint32_t o = *w;
-  for (;;) {
-    const uint32_t nw = is_min ? box_pack_min(o, x, y) : box_pack_max(o, x, y);
-    if (nw == o) return;
-    const uint32_t pr = atomicCAS(w, o, nw);
-    if (pr == o) return;
-    o = pr;
-  }
-}
-
-// One tile launch resident in the cluster's shared memory.
-__device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const TileDesc &td,
-                          ScanBox *scan_boxes, SweepCtx &cx) {
+// One tile launch resident in the cluster's shared memory; B is the staged
+// referrer-box codec.
+template <class B>
+__device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const SlotDev &slot,
+                          const TileDesc &td, ScanBox *scan_boxes, SweepCtx &cx) {
+  using BoxT = typename B::T;
   cg::cluster_group cluster = cg::this_cluster();
   SmemGeom g;
   g.x0 = td.x0;
@@ -646,34 +734,43 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
   g.C = (int)cluster.num_blocks();
   g.rank = (int)cluster.block_rank();
   g.rows_mine = g.HR > g.rank ? (g.HR - g.rank + g.C - 1) / g.C : 0;
-  const SmemTile sm = carve_smem(smem, smem_cap(td.TW, td.TH, g.C));
+  g.sh = (sizeof(BoxT) == 4 && (g.P > 256 || g.HR > 256)) ? 1 : 0;
+  const SmemTile sm = carve_smem(smem, smem_cap(td.TW, td.TH, g.C), (int)sizeof(BoxT), slot, g.rank);
+  BoxT *const sbox = (BoxT *)sm.box;
   const uint32_t lane = threadIdx.x & 31;
   const int nslots = g.rows_mine * g.P;
   const int nwords = (nslots + 31) / 32;
 
-  // ---- stage the tile and its halo (state, referrer boxes) ----
+  // ---- stage the tile and its halo (state; referrer boxes restricted to
+  // the staged region, where this launch's scans look) ----
   for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
     const int lr = s / g.P, hx = s % g.P;
     const int hy = g.rank + lr * g.C;
     const int gx = g.x0 - 1 + hx, gy = g.y0 - 1 + hy;
     float t = FLT_MAX;
-    uint32_t r = kNoRef, lo = kEmptyBox, hi = 0;
+    uint32_t r = kNoRef;
+    BoxT box = B::kEmpty;
     if (gx >= 0 && gy >= 0 && gx < j.W && gy < j.H) {
       const int64_t c = gx + (int64_t)gy * j.W;
       t = __ldcg(j.time + c);
       r = __ldcg(j.refs + c);
       const uint32_t bx0 = __ldcg(j.box_x0 + c);
       if (bx0 != kEmptyBox) {
-        lo = bx0 | (__ldcg(j.box_y0 + c) << 16);
-        hi = __ldcg(j.box_x1 + c) | (__ldcg(j.box_y1 + c) << 16);
+        const Box b = clip_box((int)bx0, (int)__ldcg(j.box_y0 + c), (int)__ldcg(j.box_x1 + c),
+                               (int)__ldcg(j.box_y1 + c), g.x0, g.y0, g.TW, g.TH, j.W, j.H);
+        if (b.x0 <= b.x1 && b.y0 <= b.y1)
+          box = B::pack(b.x0 - (g.x0 - 1), b.y0 - (g.y0 - 1), b.x1 - (g.x0 - 1), b.y1 - (g.y0 - 1),
+                        g.sh);
       }
     }
     sm.time[s] = t;
     sm.ref[s] = r;
-    sm.blo[s] = lo;
-    sm.bhi[s] = hi;
+    sbox[s] = box;
   }
-  for (int w = threadIdx.x; w < nwords; w += blockDim.x) sm.dirty[w] = 0u;
+  for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
+    sm.dirty[w] = 0u;
+    sm.grown[w] = 0u;
+  }
   if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = sm.ctr[2] = sm.ctr[3] = 0u;
   cluster.sync();
   cx.tick(3);
@@ -683,18 +780,11 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
   for (;;) {
     ++cx.sweeps;
     // ---- evaluate: this CTA's list (all its tile cells, or its marks) ----
-    if (first) {
-      for (int s0 = (int)(threadIdx.x & ~31u); s0 < nslots; s0 += blockDim.x) {
-        const int s = s0 + (int)lane;
-        bool in_tile = false;
-        if (s < nslots) {
-          const int hx = s % g.P, hy = g.rank + (s / g.P) * g.C;
-          in_tile = hx >= 1 && hx <= g.TW && hy >= 1 && hy <= g.TH;
-        }
-        const uint32_t at = warp_append(sm.ctr + 0, in_tile ? 1u : 0u, lane);
-        if (in_tile) sm.list[at] = (uint16_t)s;
-      }
-    } else {
+    // The first sweep's list is implicit: the in-tile rows of this CTA
+    // (local rows lr_first ..), TW cells each.
+    const int lr_first = g.rank == 0 ? 1 : 0;
+    const int in_rows = g.TH >= g.rank ? max((g.TH - g.rank) / g.C - lr_first + 1, 0) : 0;
+    if (!first) {
       for (int w0 = (int)(threadIdx.x & ~31u); w0 < nwords; w0 += blockDim.x) {
         const int w = w0 + (int)lane;
         uint32_t bits = 0;
@@ -703,11 +793,11 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
           if (bits) sm.dirty[w] = 0u;
         }
         uint32_t at = warp_append(sm.ctr + 0, __popc(bits), lane);
-        for (; bits; bits &= bits - 1) sm.list[at++] = (uint16_t)(w * 32 + __ffs(bits) - 1);
+        for (; bits; bits &= bits - 1) list_put(sm, at++, (uint32_t)(w * 32 + __ffs(bits) - 1));
       }
     }
     __syncthreads();
-    const uint32_t nlist = sm.ctr[0];
+    const uint32_t nlist = first ? (uint32_t)(in_rows * g.TW) : sm.ctr[0];
     if (threadIdx.x == 0) cx.cnt.evals += nlist;
     // four cells per warp, eight lanes per cell
     for (uint32_t base = (threadIdx.x >> 5) * 4; base < nlist; base += (blockDim.x >> 5) * 4) {
@@ -717,7 +807,8 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
       int x = 0, y = 0;
       Best own{FLT_MAX, kNoRef};
       if (valid) {
-        s = sm.list[ci];
+        s = first ? (uint32_t)((lr_first + (int)ci / g.TW) * g.P + 1 + (int)ci % g.TW)
+                  : list_get(sm, ci);
         const int hx = (int)s % g.P, hy = g.rank + ((int)s / g.P) * g.C;
         x = g.x0 - 1 + hx;
         y = g.y0 - 1 + hy;
@@ -726,11 +817,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
       const Best b = evaluate_coop(j, dc, SmemAcc{j, sm, g}, x, y, own, valid, lane, cx.cnt);
       const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
       const uint32_t at = warp_append(sm.ctr + 1, improved ? 1u : 0u, lane);
-      if (improved) {
-        sm.uidx[at] = (uint16_t)s;
-        sm.utime[at] = b.time;
-        sm.uref[at] = b.ref;
-      }
+      if (improved) upd_put(sm, at, s, b.time, b.ref);
     }
     __syncthreads();
     if (threadIdx.x == 0 && sm.ctr[1]) atomicAdd(rank_ptr(sm.ctr, 0) + 2 + par, sm.ctr[1]);
@@ -752,32 +839,41 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
       uint32_t want = 0;
       Box box{1, 1, 0, 0};
       if (valid) {
-        const uint32_t s = sm.uidx[u];
+        uint32_t s, r;
+        float t;
+        upd_get(sm, u, s, t, r);
         const int hx = (int)s % g.P, hy = g.rank + ((int)s / g.P) * g.C;
         const int x = g.x0 - 1 + hx, y = g.y0 - 1 + hy;
-        const uint32_t r = sm.uref[u];
-        sm.time[s] = sm.utime[u];
+        sm.time[s] = t;
         sm.ref[s] = r;
-        // referrer box of r: in shared memory inside the staged region, else
-        // in global memory
+        // referrer box of r: the staged box inside the staged region (merged
+        // into the grid-wide box at the end of the launch), else the
+        // grid-wide box in global memory
         const int rhx = ref_x(r) - (g.x0 - 1), rhy = ref_y(r) - (g.y0 - 1);
         if (rhx >= 0 && rhy >= 0 && rhx < g.P && rhy < g.HR) {
           const int owner = rhy % g.C;
           const int li = (rhy / g.C) * g.P + rhx;
-          smem_box_cas((owner == g.rank ? sm.blo : rank_ptr(sm.blo, owner)) + li, x, y, true);
-          smem_box_cas((owner == g.rank ? sm.bhi : rank_ptr(sm.bhi, owner)) + li, x, y, false);
+          // the staged box is rounded outwards, so it may hold (x, y) already
+          // while the grid-wide box does not: mark the slot for the merge
+          // either way
+          B::grow((owner == g.rank ? sbox : rank_ptr(sbox, owner)) + li, hx, hy, g.sh);
+          atomicOr((owner == g.rank ? sm.grown : rank_ptr(sm.grown, owner)) + (li >> 5),
+                   1u << (li & 31));
         } else {
           box_expand_global(j, r, x, y);
         }
         // only a burning cell is read by its neighbours
-        if (sm.utime[u] < j.max_time && __ldg(j.speed + x + (int64_t)y * j.W) != 0.0f)
+        if (t < j.max_time && __ldg(j.speed + x + (int64_t)y * j.W) != 0.0f)
           mark3x3_smem(sm, g, hx, hy);
         want = pack_ref(x, y);
-        const uint32_t lo = sm.blo[s];
-        if (lo != kEmptyBox) {
-          const uint32_t hi = sm.bhi[s];
-          box = clip_box((int)(lo & 0xFFFFu), (int)(lo >> 16), (int)(hi & 0xFFFFu), (int)(hi >> 16),
-                         g.x0, g.y0, g.TW, g.TH, j.W, j.H);
+        const BoxT pb = sbox[s];
+        if (pb != B::kEmpty) {
+          // halo-local corners back to grid cells, then clipped to the
+          // staged region and the grid
+          int bx0, by0, bx1, by1;
+          B::decode(pb, g.sh, bx0, by0, bx1, by1);
+          box = clip_box(g.x0 - 1 + bx0, g.y0 - 1 + by0, g.x0 - 1 + bx1, g.y0 - 1 + by1, g.x0, g.y0,
+                         g.TW, g.TH, j.W, j.H);
         }
       }
       warp_scan_boxes(
@@ -802,23 +898,27 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
       break;
     }
   }
-  // ---- write the tile and its halo back (halo times and references are
-  // unchanged; their referrer boxes may have grown) ----
+  // ---- write the tile's state back (halo times and references are
+  // unchanged) and merge the staged boxes that grew into the grid-wide boxes
+  // (rounded outwards: a box may cover a cell more than its referrers, which
+  // costs scan work, never a missed referrer) ----
   for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
     const int lr = s / g.P, hx = s % g.P;
     const int hy = g.rank + lr * g.C;
     const int gx = g.x0 - 1 + hx, gy = g.y0 - 1 + hy;
     if (gx < 0 || gy < 0 || gx >= j.W || gy >= j.H) continue;
     const int64_t c = gx + (int64_t)gy * j.W;
-    j.time[c] = sm.time[s];
-    j.refs[c] = sm.ref[s];
-    const uint32_t lo = sm.blo[s];
-    if (lo != kEmptyBox) {
-      const uint32_t hi = sm.bhi[s];
-      j.box_x0[c] = lo & 0xFFFFu;
-      j.box_y0[c] = lo >> 16;
-      j.box_x1[c] = hi & 0xFFFFu;
-      j.box_y1[c] = hi >> 16;
+    if (hx >= 1 && hx <= g.TW && hy >= 1 && hy <= g.TH) {
+      j.time[c] = sm.time[s];
+      j.refs[c] = sm.ref[s];
+    }
+    if (sm.grown[s >> 5] & (1u << (s & 31))) {
+      int bx0, by0, bx1, by1;
+      B::decode(sbox[s], g.sh, bx0, by0, bx1, by1);
+      atomicMin(j.box_x0 + c, (uint32_t)max(g.x0 - 1 + bx0, 0));
+      atomicMin(j.box_y0 + c, (uint32_t)max(g.y0 - 1 + by0, 0));
+      atomicMax(j.box_x1 + c, (uint32_t)min(g.x0 - 1 + bx1, j.W - 1));
+      atomicMax(j.box_y1 + c, (uint32_t)min(g.y0 - 1 + by1, j.H - 1));
     }
   }
   if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = 0u;
@@ -877,7 +977,10 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
         td.y0 = (t / j.TX) * j.T;
         td.TW = min(j.T, j.W - td.x0);
         td.TH = min(j.T, j.H - td.y0);
-        const bool w = j.smem_tile ? tile_smem(j, dc, dyn_smem, td, scan_boxes, cx)
+        const bool w = j.smem_tile == kSmemTileExact
+                           ? tile_smem<BoxExact>(j, dc, dyn_smem, s, td, scan_boxes, cx)
+                       : j.smem_tile == kSmemTileCoarse
+                           ? tile_smem<BoxCoarse>(j, dc, dyn_smem, s, td, scan_boxes, cx)
                                    : tile_global(j, dc, s, td, scan_boxes, tid, nthreads, cx);
         round_worked |= w;
       }

@@ -12,7 +12,7 @@ struct JobDev {
   int32_t T;       // tile side in cells (>= max(W, H) means one tile)
   int32_t TX, TY;  // tiles per axis
   int32_t north_up;
-  int32_t smem_tile;  // 1: tile launches run resident in the cluster's shared memory
+  int32_t smem_tile;  // kSmemTile*: where tile launches keep the tile's state
   const float *speed, *az, *ecc;
   float *time;         // state, becomes the output after the post pass
   uint32_t *refs;      // state: packed x | y << 16
@@ -34,14 +34,21 @@ struct Update {
   uint32_t pad;
 };
 
-// Global-memory scratch of one cluster slot (used by tile launches that do
-// not fit in shared memory); capacity = largest such tile area of the batch.
+// Global-memory scratch of one cluster slot.  cand/dirty/scan/upd serve tile
+// launches that do not fit in shared memory (capacity = largest such tile
+// area of the batch); ovf_list/ovf_upd take the work-list and update-list
+// entries of shared-memory tiles beyond their shared-memory capacity
+// (ovf_cap entries per CTA of the cluster, CTA r at offset r * ovf_cap).
 struct SlotDev {
   uint32_t *cand[2];
   uint32_t *dirty;
   uint32_t *scan;
   Update *upd;
   uint32_t *ctr;  // [0..1] ncand, [2] nupd, [3] nscan, [4] job
+  uint16_t *ovf_list;
+  Update *ovf_upd;
+  uint32_t ovf_cap;
+  uint32_t pad;
 };
 
 // Per-job statistics accumulated on the device (PropagStats order).
@@ -62,17 +69,33 @@ constexpr uint32_t kStatusSweepLimit = 1;
 // Shared-memory tile layout: rows of the tile plus its one-cell halo are
 // dealt to the cluster's CTAs round-robin (row hy -> CTA hy % C), so that a
 // front of any orientation spreads over all CTAs.  Bytes per cell slot:
-// time 4, reference 4, referrer box 8, work list 2, pending update 10.
-constexpr int kSmemBytesPerCell = 28;
+// time 4, reference 4, referrer box 4 (halo-local corners, one byte each,
+// in units of 1 << box_shift cells), a dirty bit and a box-grown bit.  The work list and
+// the update list hold kSmemListCap / kSmemUpdCap entries in shared memory
+// and spill beyond that to the slot's global overflow arrays.
+// With exact referrer boxes (BoxExact, 8 bytes) a slot takes 16 bytes.
+constexpr int kSmemBytesPerCell = 12;
+constexpr int kSmemBytesPerCellExact = 16;
+constexpr int kSmemListCap = 4096;  // u16 slot indices
+constexpr int kSmemUpdCap = 2048;   // u16 slot + f32 time + u32 reference
 constexpr int kSmemFixedBytes = 256;
+constexpr int kSmemMaxSide = 510;  // halo side whose corners fit a byte at box_shift 1
+
+// JobDev::smem_tile
+constexpr int32_t kSmemTileGlobal = 0;  // state in global memory, work lists in the slot
+constexpr int32_t kSmemTileCoarse = 1;  // shared memory, BoxCoarse referrer boxes
+constexpr int32_t kSmemTileExact = 2;   // shared memory, BoxExact referrer boxes
 
 __host__ __device__ inline int smem_rows_per_cta(int TH, int C) { return (TH + 2 + C - 1) / C; }
 __host__ __device__ inline int smem_cap(int TW, int TH, int C) {
   return smem_rows_per_cta(TH, C) * (TW + 2);
 }
-__host__ __device__ inline size_t smem_bytes(int TW, int TH, int C) {
+__host__ __device__ inline size_t smem_bytes(int TW, int TH, int C, bool exact = false) {
+  if (TW + 2 > kSmemMaxSide || TH + 2 > kSmemMaxSide) return ~(size_t)0;  // never fits
   const size_t cap = (size_t)smem_cap(TW, TH, C);
-  return cap * kSmemBytesPerCell + (cap / 32 + 1) * 4 + kSmemFixedBytes;
+  return cap * (exact ? kSmemBytesPerCellExact : kSmemBytesPerCell) + (cap / 32 + 1) * 8 +
+         (size_t)kSmemListCap * 2 +
+         (size_t)kSmemUpdCap * 10 + kSmemFixedBytes;
 }
 
 }  // namespace propag

@@ -5,17 +5,20 @@
 // when this module is loaded; nothing is allocated per call.  Its layout:
 //
 //   [0, 256)        JobDev of the running job
-//   [256, 512)      SlotDev (only its counters are used: tiles run in shared memory)
+//   [256, 512)      SlotDev (counters and list overflow: tiles run in shared memory)
 //   [512, 768)      StatsDev
 //   [768, 1024)     job queue counter
 //   [1024, 1280)    slot counters
 //   [2048, ...)     five per-cell arrays of kStaticMaxCells uint32 (references
 //                   and the four referrer-box corners), then the boundary
-//                   bitmap (kStaticMaxCells / 32 words)
+//                   bitmap (kStaticMaxCells / 32 words), then the overflow of
+//                   the shared-memory work and update lists
+//                   (kStaticOvfSlots u16 entries, then kStaticOvfSlots Updates)
 //
 // The per-cell arrays are initialised by the boundary/initial-state pass of
 // every call; the statistics, queue and counters are cleared by
-// stage_static_kernel at the start of every call.  Nothing needs to be zero
+// stage_static_kernel at the start of every call; list overflow entries are
+// written before they are read within a sweep.  Nothing needs to be zero
 // across calls.
 #include <cuda_runtime.h>
 
@@ -28,6 +31,8 @@ static_assert(sizeof(JobDev) <= 256, "JobDev exceeds its scratch slot");
 static_assert(sizeof(SlotDev) <= 256, "SlotDev exceeds its scratch slot");
 static_assert(sizeof(StatsDev) <= 256, "StatsDev exceeds its scratch slot");
 static_assert(kStaticMaxCells % 32 == 0, "bitmap words");
+static_assert(sizeof(Update) == 16, "overflow update entries are 16 bytes");
+static_assert(kStaticOvfUpdOff % 16 == 0, "overflow updates are 16-byte aligned");
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 

@@ -25,7 +25,13 @@ constexpr int kStaticCtrWords = 16;
 constexpr size_t kStaticCellsOff = 2048;
 constexpr size_t kStaticArrayBytes = kStaticMaxCells * 4;
 constexpr size_t kStaticBndOff = kStaticCellsOff + 5 * kStaticArrayBytes;
-constexpr size_t kStaticScratchBytes = kStaticBndOff + kStaticMaxCells / 8;
+// Overflow of the shared-memory work and update lists: cluster size x cell
+// slots per CTA entries (16 CTAs x 17 408 slots covers every tile whose
+// shared-memory footprint fits the 200 KB budget).
+constexpr size_t kStaticOvfSlots = 16 * 17408;
+constexpr size_t kStaticOvfListOff = kStaticBndOff + kStaticMaxCells / 8;
+constexpr size_t kStaticOvfUpdOff = kStaticOvfListOff + kStaticOvfSlots * 2;
+constexpr size_t kStaticScratchBytes = kStaticOvfUpdOff + kStaticOvfSlots * 16;
 
 // Device address of the scratch on the current device (cudaGetSymbolAddress).
 cudaError_t static_scratch_address(void **ptr);

@@ -91,6 +91,45 @@ def test_shared_memory_and_global_tiles(pp, oracle, cluster):
         assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
 
 
+@pytest.mark.parametrize("tile,cluster", [(300, 16), (300, 8), (323, 0)])
+def test_wide_tiles_several_launches(pp, oracle, tile, cluster):
+    """Tiles wider than 254 cells keep their staged referrer boxes at
+    two-cell granularity; over several tile launches and rounds the scans
+    must still find every referrer (exact evaluation counts)."""
+    from py_propag import scenarios as S
+    sc = S.config1(size=640, seed=17, n_ign=8, max_time=14400.0)
+    s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
+    res = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=tile, cluster=cluster)
+    sp, az, ec = _fire(pp, sc.terrain)
+    o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                         sc.ignitions, tile=tile)
+    assert res.stats["launches"] > 4
+    assert np.array_equal(res.arrival_times.view(np.uint32), o.time.view(np.uint32))
+    assert np.array_equal(res.refs_x.reshape(sc.height, sc.width), o.refs_x)
+    for k in ("rounds", "launches", "sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
+        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+
+
+@pytest.mark.parametrize("cluster", [1, 2])
+def test_shared_memory_list_overflow(pp, oracle, cluster):
+    """Hundreds of ignitions in one shared-memory tile: the first sweeps
+    produce more work-list and update-list entries than a CTA holds in
+    shared memory (4096 / 2048), so entries spill to the global overflow."""
+    from py_propag import scenarios as S
+    sc = S.config1(size=110, seed=9, n_ign=900, max_time=3000.0)
+    s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
+    res = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=-1, cluster=cluster)
+    sp, az, ec = _fire(pp, sc.terrain)
+    o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                         sc.ignitions, tile=0)
+    assert res.stats["improvements"] > 2048 * cluster
+    assert np.array_equal(res.arrival_times.view(np.uint32), o.time.view(np.uint32))
+    assert np.array_equal(res.refs_x.reshape(sc.height, sc.width), o.refs_x)
+    assert np.array_equal(res.refs_y.reshape(sc.height, sc.width), o.refs_y)
+    for k in ("sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
+        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+
+
 def test_north_up_and_staggered_ignition_times(pp, oracle):
     from py_propag import scenarios as S
     sc = S.config0(size=96, seed=4)

@@ -116,9 +116,9 @@ def test_static_rejects_jobs_beyond_its_limits(pp):
     j.width, j.height, j.dx, j.dy, j.max_time = 1025, 1024, 5.0, 5.0, 100.0
     assert lib.propag_run_device_static(C.byref(j), None, None) == L.PROPAG_ERR_INVALID
     assert "exceeds its fixed scratch of 1048576 cells" in L.last_error()
-    # a whole-grid tile of 400 x 400 cells does not fit a 16-CTA cluster
-    buf = torch.zeros(400 * 400, dtype=torch.float32, device="cuda")
-    j.width, j.height, j.tile = 400, 400, -1
+    # a whole-grid tile of 600 x 600 cells does not fit a 16-CTA cluster
+    buf = torch.zeros(600 * 600, dtype=torch.float32, device="cuda")
+    j.width, j.height, j.tile = 600, 600, -1
     j.speed_max = j.azimuth_max = j.eccentricity = j.time = buf.data_ptr()
     assert lib.propag_run_device_static(C.byref(j), None, None) == L.PROPAG_ERR_INVALID
     assert "does not fit" in L.last_error()
