@@ -199,15 +199,15 @@ __device__ __forceinline__ Best evaluate_coop(const JobDev &j, const DirConst &d
   uint32_t nr = kNoRef;
   Fire f{0.0f, 0.0f, 0.0f};
   if (valid && nx >= 0 && ny >= 0 && nx < j.W && ny < j.H) {
-    acc.cell(nx, ny, nt, nr);
+    // the three fire loads go out together with the state load (one memory
+    // round trip), whether or not the neighbour turns out to burn
     const int64_t n = nx + (int64_t)ny * j.W;
     f.speed_max = __ldg(j.speed + n);
+    f.azimuth_max = __ldg(j.az + n);
+    f.eccentricity = __ldg(j.ecc + n);
+    acc.cell(nx, ny, nt, nr);
     act = nt < j.max_time && f.speed_max != 0.0f && !(ref_x(nr) == x && ref_y(nr) == y);
-    if (act) {
-      f.azimuth_max = __ldg(j.az + n);
-      f.eccentricity = __ldg(j.ecc + n);
-      rt = acc.time_of(nr);
-    }
+    if (act) rt = acc.time_of(nr);
   }
   cnt.gat += act ? 1u : 0u;
   float offer = kInf, cand = kInf;
