@@ -172,6 +172,32 @@ int propag_engine_run(propag_engine *engine, const PropagJob *jobs, uint32_t n_j
  * Waits for the last run to finish. */
 int propag_engine_last_times(propag_engine *engine, float ms[3]);
 
+/* A batch captured as one CUDA graph: the fire pass of every job whose
+ * terrain is given (terrains[i], device pointers; terrains may be NULL to
+ * skip the fire pass, the jobs' fire rasters then being inputs), then the
+ * propagation of all n_jobs in one persistent launch.  Creating the graph
+ * runs the batch once (uncaptured) to size the graph's private scratch, then
+ * captures a second run; every launch replays it on `stream`, reading the
+ * current contents of the same buffers (so new terrains or ignition times
+ * written there take effect; new sizes or pointers need a new graph).  The
+ * job array may be freed after creation.  No counterpart in the reference
+ * (one cooperative launch per tile from the host, crates/propag/src/propag.rs:482-556). */
+typedef struct propag_graph propag_graph;
+propag_graph *propag_graph_create(const PropagOptions *opt, const PropagJob *jobs,
+                                  const PropagTerrainPtrs *terrains, uint32_t n_jobs);
+int propag_graph_launch(propag_graph *graph, void *stream);
+/* Statistics of the graph's last completed launch (synchronises `stream`). */
+int propag_graph_stats(propag_graph *graph, void *stream, PropagStats *stats);
+void propag_graph_destroy(propag_graph *graph);
+
+/* Times the batch (fire passes as in propag_graph_create, then the engine)
+ * with each cluster size whose shared memory holds every job's tile, `repeats`
+ * runs each after a warm-up run, and writes the fastest options to *best and
+ * its time to *best_ms.  Results do not depend on the cluster size (the
+ * schedule is fixed), only the speed does.  Runs on `stream` and waits. */
+int propag_autotune(const PropagJob *jobs, const PropagTerrainPtrs *terrains, uint32_t n_jobs,
+                    void *stream, int repeats, PropagOptions *best, float *best_ms);
+
 /* Allocation-free propagation of one grid.  No counterpart in the reference:
  * its propagation allocates its device buffers on every run
  * (crates/propag/src/propag.rs:420-455).

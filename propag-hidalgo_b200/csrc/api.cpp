@@ -143,6 +143,7 @@ struct propag_engine {
   size_t pinned_jobs = 0, pinned_slots = 0;
   cudaEvent_t staged = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around prep, engine, post
+  StatsDev *last_stats = nullptr;  // device statistics of the last run's jobs
 };
 
 extern "C" propag_engine *propag_engine_create(const PropagOptions *opt) {
@@ -191,6 +192,7 @@ extern "C" void propag_engine_destroy(propag_engine *e) {
   if (e->jobs_pinned) cudaFreeHost(e->jobs_pinned);
   if (e->slots_pinned) cudaFreeHost(e->slots_pinned);
   delete e;
+  cudaGetLastError();  // leave no error of the teardown to the caller's next CUDA call
 }
 
 static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, cudaStream_t stream,
@@ -327,7 +329,10 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   const size_t meta_stats = align_up(sizeof(StatsDev) * n_jobs, 256);
   CK(e->meta.reserve(meta_jobs + meta_slots + meta_stats + 256, stream));
   // staging buffers (pinned) may still be read by the previous run's copies
-  CK(cudaEventSynchronize(e->staged));
+  // (a run being captured into a graph follows a completed uncaptured run)
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(stream, &capturing));
+  if (capturing == cudaStreamCaptureStatusNone) CK(cudaEventSynchronize(e->staged));
   if (e->pinned_jobs < n_jobs) {
     if (e->jobs_pinned) cudaFreeHost(e->jobs_pinned);
     CK(cudaMallocHost(&e->jobs_pinned, sizeof(JobDev) * n_jobs));
@@ -367,21 +372,25 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   SlotDev *d_slots = e->meta.at<SlotDev>(meta_jobs);
   StatsDev *d_stats = e->meta.at<StatsDev>(meta_jobs + meta_slots);
   uint32_t *d_queue = e->meta.at<uint32_t>(meta_jobs + meta_slots + meta_stats);
+  e->last_stats = d_stats;
   CK(cudaMemcpyAsync(d_jobs, e->jobs_pinned, sizeof(JobDev) * n_jobs, cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_slots, e->slots_pinned, sizeof(SlotDev) * n_slots, cudaMemcpyHostToDevice, stream));
-  CK(cudaEventRecord(e->staged, stream));
+  // the engine's events time uncaptured runs only (an event recorded into a
+  // graph cannot be waited on or timed from the host)
+  const bool live = capturing == cudaStreamCaptureStatusNone;
+  if (live) CK(cudaEventRecord(e->staged, stream));
   CK(cudaMemsetAsync(d_stats, 0, sizeof(StatsDev) * n_jobs, stream));
   CK(cudaMemsetAsync(d_queue, 0, 4, stream));
   // ---- kernels ----
-  CK(cudaEventRecord(e->ev[0], stream));
+  if (live) CK(cudaEventRecord(e->ev[0], stream));
   CK(launch_prep(d_jobs, n_jobs, max_cells, e->sms, stream));
   CK(launch_ignite(d_jobs, n_jobs, stream));
-  CK(cudaEventRecord(e->ev[1], stream));
+  if (live) CK(cudaEventRecord(e->ev[1], stream));
   CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, smem, d_queue, d_stats,
                    1ull << 40, stream));
-  CK(cudaEventRecord(e->ev[2], stream));
+  if (live) CK(cudaEventRecord(e->ev[2], stream));
   CK(launch_post(d_jobs, n_jobs, max_cells, e->sms, d_stats, stream));
-  CK(cudaEventRecord(e->ev[3], stream));
+  if (live) CK(cudaEventRecord(e->ev[3], stream));
   e->stream = stream;
   if (stats) {
     std::vector<StatsDev> hs(n_jobs);
@@ -423,6 +432,187 @@ extern "C" int propag_engine_last_times(propag_engine *e, float ms[3]) {
   CK(cudaSetDevice(e->device));
   CK(cudaEventSynchronize(e->ev[3]));
   for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms[i], e->ev[i], e->ev[i + 1]));
+  return PROPAG_OK;
+}
+
+// ================================================ batches as CUDA graphs ==
+static int fire_device(bool full, uint64_t n, const PropagTerrainPtrs *t, float *const outs[10],
+                       cudaStream_t stream);
+
+// The fire passes of the jobs that have a terrain, then the batch's
+// propagation (prep, ignition, engine, post), on one stream.
+static int batch_step(propag_engine *e, const PropagJob *jobs, const PropagTerrainPtrs *terrains,
+                      uint32_t n_jobs, cudaStream_t stream, PropagStats *stats) {
+  if (terrains) {
+    for (uint32_t i = 0; i < n_jobs; ++i) {
+      float *outs[10] = {nullptr, nullptr, nullptr, nullptr,
+                         const_cast<float *>(jobs[i].speed_max), const_cast<float *>(jobs[i].azimuth_max),
+                         const_cast<float *>(jobs[i].eccentricity), nullptr, nullptr, nullptr};
+      const int rc = fire_device(false, (uint64_t)jobs[i].width * jobs[i].height, terrains + i, outs, stream);
+      if (rc) return rc;
+    }
+  }
+  return engine_run(e, jobs, n_jobs, stream, stats);
+}
+
+struct propag_graph {
+  propag_engine *eng = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t n_jobs = 0;
+};
+
+extern "C" void propag_graph_destroy(propag_graph *g) {
+  if (!g) return;
+  if (g->eng) cudaSetDevice(g->eng->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  propag_engine_destroy(g->eng);
+  delete g;
+  cudaGetLastError();  // leave no error of the teardown to the caller's next CUDA call
+}
+
+extern "C" propag_graph *propag_graph_create(const PropagOptions *opt, const PropagJob *jobs,
+                                             const PropagTerrainPtrs *terrains, uint32_t n_jobs) {
+  if (!jobs || n_jobs == 0) {
+    fail(PROPAG_ERR_INVALID, "propag_graph_create: no jobs");
+    return nullptr;
+  }
+  auto *g = new propag_graph();
+  g->n_jobs = n_jobs;
+  g->eng = propag_engine_create(opt);
+  if (!g->eng) {
+    delete g;
+    return nullptr;
+  }
+  auto bail = [&](cudaError_t err, const char *what) -> propag_graph * {
+    if (err != cudaSuccess) cuda_fail(err, what);
+    propag_graph_destroy(g);
+    return nullptr;
+  };
+  cudaError_t err = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (err != cudaSuccess) return bail(err, "cudaStreamCreateWithFlags");
+  // an uncaptured run first: it sizes and allocates the engine's scratch, so
+  // that the captured run allocates nothing (and checks the jobs)
+  if (batch_step(g->eng, jobs, terrains, n_jobs, g->stream, nullptr)) return bail(cudaSuccess, "");
+  err = cudaStreamSynchronize(g->stream);
+  if (err != cudaSuccess) return bail(err, "cudaStreamSynchronize");
+  err = cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) return bail(err, "cudaStreamBeginCapture");
+  const int rc = batch_step(g->eng, jobs, terrains, n_jobs, g->stream, nullptr);
+  const std::string msg = rc ? g_error : std::string();
+  err = cudaStreamEndCapture(g->stream, &g->graph);
+  if (rc) {
+    g_error = msg;
+    return bail(cudaSuccess, "");
+  }
+  if (err != cudaSuccess) return bail(err, "cudaStreamEndCapture");
+  err = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (err != cudaSuccess) return bail(err, "cudaGraphInstantiate");
+  return g;
+}
+
+extern "C" int propag_graph_launch(propag_graph *g, void *stream) {
+  if (!g || !g->exec) return fail(PROPAG_ERR_INVALID, "null graph");
+  CK(cudaSetDevice(g->eng->device));
+  CK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  return PROPAG_OK;
+}
+
+static void to_stats(const StatsDev &h, PropagStats &o) {
+  o.rounds = h.rounds;
+  o.launches = h.launches;
+  o.sweeps = h.sweeps;
+  o.evaluations = h.evaluations;
+  o.improvements = h.improvements;
+  o.dda_steps = h.dda_steps;
+  o.gathers = h.gathers;
+  o.refbox_scans = h.refbox_scans;
+  o.burned = h.burned;
+  o.cyc_first = h.cyc_first;
+  o.cyc_eval = h.cyc_eval;
+  o.cyc_commit = h.cyc_commit;
+  o.cyc_stage = h.cyc_stage;
+  o.status = h.status;
+  o.max_walk = h.max_walk;
+  o.t_start_ns = h.t_start_ns;
+  o.t_done_ns = h.t_done_ns;
+}
+
+extern "C" int propag_graph_stats(propag_graph *g, void *stream, PropagStats *stats) {
+  if (!g || !stats) return fail(PROPAG_ERR_INVALID, "null argument");
+  propag_engine *e = g->eng;
+  if (!e->last_stats) return fail(PROPAG_ERR_INVALID, "the graph has not run");
+  CK(cudaSetDevice(e->device));
+  std::vector<StatsDev> hs(g->n_jobs);
+  CK(cudaMemcpyAsync(hs.data(), e->last_stats, sizeof(StatsDev) * g->n_jobs, cudaMemcpyDeviceToHost,
+                     (cudaStream_t)stream));
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  for (uint32_t i = 0; i < g->n_jobs; ++i) to_stats(hs[i], stats[i]);
+  for (uint32_t i = 0; i < g->n_jobs; ++i)
+    if (hs[i].status) return fail(PROPAG_ERR_TIMEOUT, "job " + std::to_string(i) + ": sweep limit reached");
+  return PROPAG_OK;
+}
+
+// ============================================================ autotuner ===
+extern "C" int propag_autotune(const PropagJob *jobs, const PropagTerrainPtrs *terrains,
+                               uint32_t n_jobs, void *stream_ptr, int repeats, PropagOptions *best,
+                               float *best_ms) {
+  if (!jobs || n_jobs == 0 || !best) return fail(PROPAG_ERR_INVALID, "propag_autotune: no jobs or output");
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  repeats = std::max(repeats, 1);
+  // candidates: cluster sizes whose shared memory holds every job's tile
+  std::vector<int> cands;
+  for (int c = 16; c >= 1; c /= 2) {
+    bool all = true;
+    for (uint32_t i = 0; i < n_jobs && all; ++i) {
+      int T = jobs[i].tile ? jobs[i].tile : PROPAG_DEFAULT_TILE;
+      if (T == PROPAG_TILE_WHOLE_GRID || T <= 0) T = (int)std::max(jobs[i].width, jobs[i].height);
+      all = smem_bytes(std::min<int>(T, (int)jobs[i].width), std::min<int>(T, (int)jobs[i].height), c) <=
+            200 * 1024;
+    }
+    if (all) cands.push_back(c);
+  }
+  if (cands.empty()) cands.push_back(16);  // global-memory tiles: the largest cluster
+  cudaEvent_t a = nullptr, b = nullptr;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  float best_t = -1.0f;
+  for (int c : cands) {
+    PropagOptions o{0, c, 0, -1};
+    propag_engine *e = propag_engine_create(&o);
+    if (!e) {
+      rc = PROPAG_ERR_CUDA;
+      break;
+    }
+    rc = batch_step(e, jobs, terrains, n_jobs, stream, nullptr);  // warm-up, allocations
+    float t_min = -1.0f;
+    for (int r = 0; r < repeats && !rc; ++r) {
+      cudaEventRecord(a, stream);
+      rc = batch_step(e, jobs, terrains, n_jobs, stream, nullptr);
+      cudaEventRecord(b, stream);
+      float ms = 0.0f;
+      if (!rc && cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess)
+        t_min = t_min < 0 ? ms : std::min(t_min, ms);
+    }
+    propag_engine_destroy(e);
+    if (rc) break;
+    if (t_min >= 0 && (best_t < 0 || t_min < best_t)) {
+      best_t = t_min;
+      *best = o;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
+  if (best_t < 0) return fail(PROPAG_ERR_CUDA, "propag_autotune: no candidate could be timed");
+  if (best_ms) *best_ms = best_t;
   return PROPAG_OK;
 }
 

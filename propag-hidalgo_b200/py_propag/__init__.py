@@ -465,6 +465,62 @@ class Engine:
             pass
 
 
+class Graph:
+    """A batch (fire passes + one persistent propagation launch) captured as
+    a CUDA graph (propag_graph_*).  ``jobs``: ``PropagJob`` structures with
+    device pointers; ``terrains``: one ``PropagTerrainPtrs`` (device) per job,
+    or None when the fire rasters are inputs."""
+
+    def __init__(self, jobs, terrains=None, tile=None, cluster=0, threads=0, device=-1):
+        lib = L.lib()
+        n = len(jobs)
+        self.n = n
+        arr = (L.PropagJob * n)(*jobs)
+        tarr = (L.PropagTerrainPtrs * n)(*terrains) if terrains is not None else None
+        opt = _options(tile, cluster, threads, device)
+        self._h = lib.propag_graph_create(C.byref(opt), arr, tarr, n)
+        if not self._h:
+            _raise(L.PROPAG_ERR_CUDA, "propag_graph_create")
+
+    def launch(self, stream=0):
+        rc = L.lib().propag_graph_launch(self._h, C.c_void_p(int(stream)))
+        if rc != 0:
+            _raise(rc, "propag_graph_launch")
+
+    def stats(self, stream=0):
+        st = (L.PropagStats * self.n)()
+        rc = L.lib().propag_graph_stats(self._h, C.c_void_p(int(stream)), st)
+        if rc != 0:
+            _raise(rc, "propag_graph_stats")
+        return [s.as_dict() for s in st]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().propag_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(jobs, terrains=None, stream=0, repeats=1):
+    """Fastest cluster size for this batch (propag_autotune): returns
+    (options dict, milliseconds)."""
+    n = len(jobs)
+    arr = (L.PropagJob * n)(*jobs)
+    tarr = (L.PropagTerrainPtrs * n)(*terrains) if terrains is not None else None
+    best = L.PropagOptions()
+    ms = C.c_float()
+    rc = L.lib().propag_autotune(arr, tarr, n, C.c_void_p(int(stream)), int(repeats), C.byref(best),
+                                 C.byref(ms))
+    if rc != 0:
+        _raise(rc, "propag_autotune")
+    return {"tile": best.tile, "cluster": best.cluster, "threads": best.threads}, float(ms.value)
+
+
 def build(force: bool = False) -> str:
     """Compiles libpropag.so for sm_100a with nvcc (make in csrc/)."""
     if force and os.path.exists(L.LIB_PATH):
@@ -479,5 +535,5 @@ __all__ = [
     "PropagResults", "PyPropagResults", "propagate", "load_terrain_data", "check_cuda_available",
     "PropagCudaError", "PropagGdalError", "PropagValidationError", "PropagMPIError",
     "fire_behaviour", "propagate_arrays", "rasterize_ignitions", "write_geotiff", "point_wkb",
-    "demo_terrain", "Engine", "build",
+    "demo_terrain", "Engine", "Graph", "autotune", "build",
 ]

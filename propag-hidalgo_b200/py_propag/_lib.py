@@ -163,6 +163,14 @@ SIGNATURES = {
     "propag_engine_run": (C.c_int, [C.c_void_p, C.POINTER(PropagJob), C.c_uint32, C.c_void_p,
                                     C.POINTER(PropagStats)]),
     "propag_engine_last_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float * 3)]),
+    "propag_graph_create": (C.c_void_p, [C.POINTER(PropagOptions), C.POINTER(PropagJob),
+                                         C.POINTER(PropagTerrainPtrs), C.c_uint32]),
+    "propag_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "propag_graph_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PropagStats)]),
+    "propag_graph_destroy": (None, [C.c_void_p]),
+    "propag_autotune": (C.c_int, [C.POINTER(PropagJob), C.POINTER(PropagTerrainPtrs), C.c_uint32,
+                                  C.c_void_p, C.c_int, C.POINTER(PropagOptions),
+                                  C.POINTER(C.c_float)]),
     "propag_run_device_static": (C.c_int, [C.POINTER(PropagJob), C.c_void_p, C.POINTER(PropagStats)]),
     "propag_run_host": (C.c_int, [C.POINTER(Settings), C.POINTER(PropagTerrainPtrs),
                                   C.POINTER(PropagIgnition), C.c_uint64, C.POINTER(PropagOptions),
