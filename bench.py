@@ -8,10 +8,12 @@ roads, smooth random wind 0-15 m/s, per-cell moisture jitter, 20 ignitions,
 max_time 43200 s), seeded synthetic inputs.  A step = fire behaviour over
 every cell + boundaries + propagation + post mask for that scenario.
 
-Batched leg (``batched`` in the JSON line): the 256-member ensemble on a
-shared 1024 x 1024 terrain (per-member wind, dead moisture and ignition,
-max_time 21600 s); all members in one persistent launch against the same
-members run one by one through the plain path, with per-scenario latency.
+Batched legs: ``batched`` -- the 256-member ensemble on a shared 1024 x 1024
+terrain (per-member wind, dead moisture and ignition, max_time 21600 s);
+``batched_uneven`` -- 64 independent scenarios, square grids 128..2048 at
+5-30 m with their own terrain.  Each: all jobs in one persistent launch
+captured as a CUDA graph (cluster size from the autotuner), against the same
+jobs run one by one through the plain path, with per-scenario latency.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
   python bench.py --impl reference ...   # the CPU implementation of the path
@@ -209,112 +211,141 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def ensemble_leg(lib, L, dev, stream, n_members: int, steps: int, warmup: int,
-                 plain_members: int) -> dict:
-    """The 256-member ensemble on a shared 1024 x 1024 terrain: every member's
-    fire pass plus ONE persistent engine launch for all members, against the
-    plain path (fire + a one-job engine run per member, one after another)."""
+def _device_jobs(L, dev, items):
+    """items: (width, height, dx, dy, max_time, tile, ignitions, terrain tensors).
+    Returns the jobs, their terrain pointer structs and the buffers that keep
+    them alive (terrain, fire rasters, ignitions, time, refs_x, refs_y, bits)."""
+    import torch
+    jobs, terrains, keep = [], [], []
+    for (w, h, dx, dy, max_time, tile, ignitions, t) in items:
+        n = w * h
+        fire = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
+        ign = np.array(list(ignitions), dtype=[("x", "<u4"), ("y", "<u4"), ("t", "<f4")])
+        ign_d = torch.from_numpy(np.frombuffer(ign.tobytes() or bytes(12), np.uint8).copy()).to(dev)
+        out = torch.empty(n, dtype=torch.float32, device=dev)
+        rx = torch.empty(n, dtype=torch.int16, device=dev)
+        ry = torch.empty(n, dtype=torch.int16, device=dev)
+        bnd = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+        j = L.PropagJob()
+        j.width, j.height, j.dx, j.dy, j.max_time, j.tile = w, h, dx, dy, max_time, tile
+        j.speed_max, j.azimuth_max, j.eccentricity = (f.data_ptr() for f in fire)
+        j.ignitions, j.n_ignitions = ign_d.data_ptr(), len(ign)
+        j.time, j.refs_x, j.refs_y, j.boundaries = out.data_ptr(), rx.data_ptr(), ry.data_ptr(), bnd.data_ptr()
+        jobs.append(j)
+        terrains.append(L.PropagTerrainPtrs(*[t[k].data_ptr() for k in L.TERRAIN_FIELDS]))
+        keep.append((t, fire, ign_d, out, rx, ry, bnd))
+    return jobs, terrains, keep
+
+
+def ensemble_batch(L, dev, n_members):
+    """The ensemble on a shared 1024 x 1024 terrain: per-member wind speed and
+    direction, dead moisture offset and ignition, max_time 21600 s."""
     import torch
     from py_propag import scenarios as S
     base, members = S.config2(n=n_members)
     N = base.width * base.height
-    words = (N + 31) // 32
-    sptr = C.c_void_p(stream.cuda_stream)
     bt = {k: torch.from_numpy(np.ascontiguousarray(v).ravel()).to(dev) for k, v in base.terrain.items()}
-    jobs, keep = [], []
+    items = []
     for m in members:
         t = dict(bt)
         t["wind_speed"] = torch.full((N,), m["wind_speed"], dtype=torch.float32, device=dev)
         t["wind_azimuth"] = torch.full((N,), m["wind_azimuth"], dtype=torch.float32, device=dev)
         for k in ("d1hr", "d10hr", "d100hr"):
             t[k] = bt[k] + np.float32(m["dead_offset"])
-        ptrs = L.PropagTerrainPtrs(*[t[k].data_ptr() for k in L.TERRAIN_FIELDS])
-        fire = [torch.empty(N, dtype=torch.float32, device=dev) for _ in range(3)]
-        ign = np.array([m["ignition"]], dtype=[("x", "<u4"), ("y", "<u4"), ("t", "<f4")])
-        ign_d = torch.from_numpy(np.frombuffer(ign.tobytes(), np.uint8).copy()).to(dev)
-        out = torch.empty(N, dtype=torch.float32, device=dev)
-        rx = torch.empty(N, dtype=torch.int16, device=dev)
-        ry = torch.empty(N, dtype=torch.int16, device=dev)
-        bnd = torch.empty(words, dtype=torch.int32, device=dev)
-        j = L.PropagJob()
-        j.width, j.height, j.dx, j.dy = base.width, base.height, base.dx, base.dy
-        j.max_time, j.tile = m["max_time"], 0
-        j.speed_max, j.azimuth_max, j.eccentricity = (f.data_ptr() for f in fire)
-        j.ignitions, j.n_ignitions = ign_d.data_ptr(), 1
-        j.time, j.refs_x, j.refs_y, j.boundaries = out.data_ptr(), rx.data_ptr(), ry.data_ptr(), bnd.data_ptr()
-        jobs.append(j)
-        keep.append((t, ptrs, fire, ign_d, out, rx, ry, bnd))
-    arr = (L.PropagJob * len(jobs))(*jobs)
+        items.append((base.width, base.height, base.dx, base.dy, m["max_time"], 0, [m["ignition"]], t))
+    desc = (f"config2: {n_members}-member ensemble on a shared {base.width}x{base.height} terrain, "
+            f"per-member wind/moisture/ignition, max_time 21600 s")
+    return _device_jobs(L, dev, items), desc
+
+
+def uneven_batch(L, dev, n):
+    """Independent scenarios of uneven sizes: square grids log-uniform in
+    128..2048 at 5-30 m, own terrain and fuel, 1-10 ignitions, 1-12 h."""
+    import torch
+    from py_propag import scenarios as S
+    scs = S.config3(n=n)
+    items = []
+    for sc in scs:
+        t = {k: torch.from_numpy(np.ascontiguousarray(v).ravel()).to(dev) for k, v in sc.terrain.items()}
+        items.append((sc.width, sc.height, sc.dx, sc.dy, sc.max_time, 0, sc.ignitions, t))
+    cells = sum(sc.width * sc.height for sc in scs)
+    desc = (f"config3: {n} scenarios, square grids {min(s.width for s in scs)}.."
+            f"{max(s.width for s in scs)} at 5-30 m ({cells / 1e6:.1f} M cells), own terrain, "
+            f"1-10 ignitions, max_time 1-12 h")
+    return _device_jobs(L, dev, items), desc
+
+
+def batched_leg(lib, L, pp, stream, batch, desc, steps, warmup, plain_jobs) -> dict:
+    """All jobs of a batch in one persistent launch, captured as a CUDA graph
+    with the cluster size the autotuner picks, against the plain path: each
+    job alone (its fire pass + a one-job engine run), one after another."""
+    import torch
+    jobs, terrains, keep = batch
+    sptr = C.c_void_p(stream.cuda_stream)
     eng = lib.propag_engine_create(C.byref(L.PropagOptions(0, 0, 0, -1)))
     if not eng:
         raise RuntimeError(L.last_error())
+    arr = (L.PropagJob * len(jobs))(*jobs)
 
-    def fire(i):
-        f = keep[i][2]
-        if lib.propag_fire_simple_device(N, C.byref(keep[i][1]), f[0].data_ptr(), f[1].data_ptr(),
-                                         f[2].data_ptr(), sptr):
+    def plain_one(i):
+        j = jobs[i]
+        if lib.propag_fire_simple_device(j.width * j.height, C.byref(terrains[i]), j.speed_max,
+                                         j.azimuth_max, j.eccentricity, sptr):
+            raise RuntimeError(L.last_error())
+        p = C.cast(C.addressof(arr) + i * C.sizeof(L.PropagJob), C.POINTER(L.PropagJob))
+        if lib.propag_engine_run(eng, p, 1, sptr, None):
             raise RuntimeError(L.last_error())
 
-    def run(first, count, stats=None):
-        p = C.cast(C.addressof(arr) + first * C.sizeof(L.PropagJob), C.POINTER(L.PropagJob))
-        if lib.propag_engine_run(eng, p, count, sptr, stats):
-            raise RuntimeError(L.last_error())
-
-    def batched_step(stats=None):
-        for i in range(len(jobs)):
-            fire(i)
-        run(0, len(jobs), stats)
-
-    # plain path: each member alone, in order (its own latency is its time)
-    plain_members = min(plain_members, len(jobs))
+    plain_jobs = min(plain_jobs, len(jobs))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    fire(0)
-    run(0, 1)
+    plain_one(0)
     torch.cuda.synchronize()
     plain_ms, plain_out = [], []
-    for i in range(plain_members):
+    for i in range(plain_jobs):
         e0.record(stream)
-        fire(i)
-        run(i, 1)
+        plain_one(i)
         e1.record(stream)
         torch.cuda.synchronize()
         plain_ms.append(e0.elapsed_time(e1))
-        plain_out.append(keep[i][4].clone())
-    # batched: all members in one launch
-    st = (L.PropagStats * len(jobs))()
-    batched_step(st)  # first run: statistics and per-member device timestamps
+        plain_out.append(keep[i][3].clone())
+    lib.propag_engine_destroy(eng)
+    # batched: autotuned cluster size, one CUDA graph replayed per batch
+    best, tune_ms = pp.autotune(jobs, terrains, stream=stream.cuda_stream, repeats=1)
+    g = pp.Graph(jobs, terrains, cluster=best["cluster"])
     for _ in range(warmup):
-        batched_step()
+        g.launch(stream.cuda_stream)
     torch.cuda.synchronize()
     step_ms = []
     for _ in range(steps):
         e0.record(stream)
-        batched_step()
+        g.launch(stream.cuda_stream)
         e1.record(stream)
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
-    same = all(torch.equal(plain_out[i], keep[i][4]) for i in range(plain_members))
-    t0 = min(s.t_start_ns for s in st)
-    fire_prep_ms = float(np.median(step_ms)) - (max(s.t_done_ns for s in st) - t0) / 1e6
-    lat = np.array([(s.t_done_ns - t0) / 1e6 + max(fire_prep_ms, 0.0) for s in st])
-    lib.propag_engine_destroy(eng)
-    batched = len(jobs) / (float(np.median(step_ms)) / 1e3)
+    st = g.stats(stream.cuda_stream)
+    g.close()
+    same = all(torch.equal(plain_out[i], keep[i][3]) for i in range(plain_jobs))
+    t0 = min(s["t_start_ns"] for s in st)
+    batch_ms = float(np.median(step_ms))
+    fire_prep_ms = batch_ms - (max(s["t_done_ns"] for s in st) - t0) / 1e6
+    lat = np.array([(s["t_done_ns"] - t0) / 1e6 + max(fire_prep_ms, 0.0) for s in st])
+    batched = len(jobs) / (batch_ms / 1e3)
     plain = len(plain_ms) / (float(np.sum(plain_ms)) / 1e3)
     return {
-        "workload": f"config2: {len(jobs)}-member ensemble on a shared {base.width}x{base.height} "
-                    f"terrain, per-member wind/moisture/ignition, max_time 21600 s",
-        "value": batched, "unit": UNIT, "ms_per_batch": float(np.median(step_ms)),
+        "workload": desc, "value": batched, "unit": UNIT, "ms_per_batch": batch_ms,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "note": "batch start to each member's propagation end (device clock), "
+                       "note": "batch start to each job's propagation end (device clock), "
                                "plus the batch's fire/prep time"},
-        "plain": {"value": plain, "unit": UNIT, "members_timed": len(plain_ms),
+        "plain": {"value": plain, "unit": UNIT, "jobs_timed": len(plain_ms),
                   "latency_ms": {"p50": float(np.percentile(plain_ms, 50)),
                                  "p99": float(np.percentile(plain_ms, 99))}},
         "speedup_vs_plain": batched / plain,
         "matches_plain_bitwise": bool(same),
+        "graph": "fire passes + one persistent propagation launch, captured once, replayed per batch",
+        "autotuned": {"cluster": best["cluster"], "tuning_ms": tune_ms},
         "gpu_launches_per_batch": len(jobs) + 4,
-        "sweeps_mean": float(np.mean([s.sweeps for s in st])),
-        "evaluations": int(sum(s.evaluations for s in st)),
+        "sweeps_mean": float(np.mean([s["sweeps"] for s in st])),
+        "evaluations": int(sum(s["evaluations"] for s in st)),
     }
 
 
@@ -329,7 +360,8 @@ def main():
     ap.add_argument("--cluster", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--ensemble", type=int, default=256, help="members of the batched leg (0 = skip)")
+    ap.add_argument("--ensemble", type=int, default=256, help="members of the ensemble leg (0 = skip)")
+    ap.add_argument("--uneven", type=int, default=64, help="scenarios of the uneven leg (0 = skip)")
     ap.add_argument("--plain-members", type=int, default=256,
                     help="ensemble members timed one by one on the plain path")
     args = ap.parse_args()
@@ -473,8 +505,15 @@ def bench_b200(args):
     lib.propag_engine_destroy(eng)
     del t_dev, fire, time_d, rx_d, ry_d, bnd_d
     if args.ensemble > 0:
-        line["batched"] = ensemble_leg(lib, L, dev, stream, args.ensemble, args.steps, args.warmup,
-                                       args.plain_members)
+        batch, bdesc = ensemble_batch(L, dev, args.ensemble)
+        line["batched"] = batched_leg(lib, L, pp, stream, batch, bdesc, args.steps, args.warmup,
+                                      args.plain_members)
+        del batch
+    if args.uneven > 0:
+        batch, bdesc = uneven_batch(L, dev, args.uneven)
+        line["batched_uneven"] = batched_leg(lib, L, pp, stream, batch, bdesc, args.steps,
+                                             args.warmup, args.uneven)
+        del batch
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(sc, stats["evaluations"], os.cpu_count() or 1)
     if world > 1:
