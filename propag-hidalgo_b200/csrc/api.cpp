@@ -35,7 +35,8 @@ cudaError_t launch_prep(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells,
 cudaError_t launch_ignite(const JobDev *jobs, uint32_t n_jobs, cudaStream_t stream);
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
                           uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
-                          StatsDev *stats, unsigned long long max_sweeps, cudaStream_t stream);
+                          StatsDev *stats, unsigned long long max_sweeps, const uint32_t *order,
+                          cudaStream_t stream);
 cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n);
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
                         StatsDev *stats, cudaStream_t stream);
@@ -327,7 +328,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   const size_t meta_jobs = align_up(sizeof(JobDev) * n_jobs, 256);
   const size_t meta_slots = align_up(sizeof(SlotDev) * n_slots, 256);
   const size_t meta_stats = align_up(sizeof(StatsDev) * n_jobs, 256);
-  CK(e->meta.reserve(meta_jobs + meta_slots + meta_stats + 256, stream));
+  const size_t meta_order = align_up(sizeof(uint32_t) * n_jobs, 256);
+  CK(e->meta.reserve(meta_jobs + meta_slots + meta_stats + 256 + meta_order, stream));
   // staging buffers (pinned) may still be read by the previous run's copies
   // (a run being captured into a graph follows a completed uncaptured run)
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
@@ -335,7 +337,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   if (capturing == cudaStreamCaptureStatusNone) CK(cudaEventSynchronize(e->staged));
   if (e->pinned_jobs < n_jobs) {
     if (e->jobs_pinned) cudaFreeHost(e->jobs_pinned);
-    CK(cudaMallocHost(&e->jobs_pinned, sizeof(JobDev) * n_jobs));
+    // the job descriptors, then the queue order
+    CK(cudaMallocHost(&e->jobs_pinned, sizeof(JobDev) * n_jobs + sizeof(uint32_t) * n_jobs));
     e->pinned_jobs = n_jobs;
   }
   if (e->pinned_slots < n_slots) {
@@ -344,6 +347,13 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     e->pinned_slots = n_slots;
   }
   std::copy(jd.begin(), jd.end(), e->jobs_pinned);
+  // queue order: largest grids first, so that the longest jobs start first
+  // and the batch ends close to its longest job (results do not depend on it)
+  uint32_t *order_pinned = reinterpret_cast<uint32_t *>(e->jobs_pinned + n_jobs);
+  for (uint32_t i = 0; i < n_jobs; ++i) order_pinned[i] = i;
+  std::stable_sort(order_pinned, order_pinned + n_jobs, [&](uint32_t a, uint32_t b) {
+    return (uint64_t)jd[a].W * jd[a].H > (uint64_t)jd[b].W * jd[b].H;
+  });
   for (uint32_t s = 0; s < n_slots; ++s) {
     size_t o = slot_bytes * s;
     SlotDev &sd = e->slots_pinned[s];
@@ -372,8 +382,10 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   SlotDev *d_slots = e->meta.at<SlotDev>(meta_jobs);
   StatsDev *d_stats = e->meta.at<StatsDev>(meta_jobs + meta_slots);
   uint32_t *d_queue = e->meta.at<uint32_t>(meta_jobs + meta_slots + meta_stats);
+  uint32_t *d_order = e->meta.at<uint32_t>(meta_jobs + meta_slots + meta_stats + 256);
   e->last_stats = d_stats;
   CK(cudaMemcpyAsync(d_jobs, e->jobs_pinned, sizeof(JobDev) * n_jobs, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_order, order_pinned, sizeof(uint32_t) * n_jobs, cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_slots, e->slots_pinned, sizeof(SlotDev) * n_slots, cudaMemcpyHostToDevice, stream));
   // the engine's events time uncaptured runs only (an event recorded into a
   // graph cannot be waited on or timed from the host)
@@ -387,7 +399,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   CK(launch_ignite(d_jobs, n_jobs, stream));
   if (live) CK(cudaEventRecord(e->ev[1], stream));
   CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, smem, d_queue, d_stats,
-                   1ull << 40, stream));
+                   1ull << 40, d_order, stream));
   if (live) CK(cudaEventRecord(e->ev[2], stream));
   CK(launch_post(d_jobs, n_jobs, max_cells, e->sms, d_stats, stream));
   if (live) CK(cudaEventRecord(e->ev[3], stream));
@@ -715,7 +727,8 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   CK(launch_stage_static(d_job, d, d_slot, s, d_stats, d_queue, stream));
   CK(launch_prep(d_job, 1, N, sms, stream));
   CK(launch_ignite(d_job, 1, stream));
-  CK(launch_engine(d_job, 1, d_slot, 1, csize, engine_threads(), smem, d_queue, d_stats, 1ull << 40, stream));
+  CK(launch_engine(d_job, 1, d_slot, 1, csize, engine_threads(), smem, d_queue, d_stats, 1ull << 40,
+                   nullptr, stream));
   CK(launch_post(d_job, 1, N, sms, d_stats, stream));
   if (stats) {
     StatsDev h;

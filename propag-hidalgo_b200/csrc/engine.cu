@@ -933,7 +933,8 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
                                                          const SlotDev *__restrict__ slots,
                                                          uint32_t *__restrict__ queue,
                                                          StatsDev *__restrict__ stats,
-                                                         unsigned long long max_sweeps) {
+                                                         unsigned long long max_sweeps,
+                                                         const uint32_t *__restrict__ order) {
   extern __shared__ __align__(16) char dyn_smem[];
   cg::cluster_group cluster = cg::this_cluster();
   const uint32_t csize = cluster.num_blocks();
@@ -952,8 +953,11 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
       s.ctr[0] = s.ctr[1] = s.ctr[2] = s.ctr[3] = 0;
     }
     sync_cluster();
-    const uint32_t jid = __ldcg(s.ctr + 4);
-    if (jid >= n_jobs) return;
+    // clusters take the jobs in queue order; `order` (when given) maps queue
+    // positions to jobs, e.g. largest first so that the longest jobs start early
+    const uint32_t q = __ldcg(s.ctr + 4);
+    if (q >= n_jobs) return;
+    const uint32_t jid = order ? __ldg(order + q) : q;
     if (threadIdx.x == 0) {
       js = jobs[jid];
       dir_consts(js, dc);
@@ -1096,12 +1100,13 @@ cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n) {
 
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
                           uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
-                          StatsDev *stats, unsigned long long max_sweeps, cudaStream_t stream) {
+                          StatsDev *stats, unsigned long long max_sweeps, const uint32_t *order,
+                          cudaStream_t stream) {
   cudaError_t e = engine_attrs(smem);
   if (e != cudaSuccess) return e;
   cudaLaunchAttribute attr[1];
   cudaLaunchConfig_t cfg = engine_config(csize, threads, n_slots * (unsigned)csize, smem, attr, stream);
-  return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps);
+  return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps, order);
 }
 
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
