@@ -172,6 +172,56 @@ int propag_engine_run(propag_engine *engine, const PropagJob *jobs, uint32_t n_j
  * Waits for the last run to finish. */
 int propag_engine_last_times(propag_engine *engine, float ms[3]);
 
+/* Statistics of the jobs of the engine's last propag_engine_run (its first
+ * n_jobs jobs; n_jobs at most that run's count), for runs made without
+ * `stats`: copies on `stream` and synchronises it. */
+int propag_engine_last_stats(propag_engine *engine, void *stream, PropagStats *stats,
+                             uint32_t n_jobs);
+
+/* ---- serving: continuous batching ------------------------------------------
+ * A server owns `lanes` CUDA streams, each with its own engine, and a
+ * dispatcher thread.  propag_server_submit queues one scenario (device
+ * pointers, like PropagJob; `terrain` optional: with it the fire pass runs
+ * first and writes the job's fire rasters).  Whenever a lane is free the
+ * dispatcher takes the requests waiting at that moment, up to max_batch and
+ * within hbm_budget bytes of device memory in flight (each request counts
+ * `device_bytes`, 64 B per cell when 0), and runs them as one batch on that
+ * lane; requests that arrive while batches are on the GPU are admitted as
+ * lanes and memory free up, and run alongside them.  A request's results are
+ * the same alone and in any batch.  No counterpart in the reference (one
+ * synchronous propagation per call, crates/propag/src/propag.rs:323-574). */
+typedef struct PropagServerOptions {
+  uint64_t hbm_budget; /* bytes of device memory in flight; 0 = no limit */
+  uint32_t lanes;      /* batches in flight at once (streams); 0 = 4 */
+  uint32_t max_batch;  /* requests per batch; 0 = 64 */
+  int32_t device;      /* CUDA device ordinal; -1 = the current device */
+  int32_t pad;
+} PropagServerOptions;
+
+typedef struct PropagServerResult {
+  PropagStats stats;
+  uint64_t submit_ns, start_ns, done_ns; /* host steady clock: queued, dispatched, seen done */
+  int32_t status;                        /* 0 queued or running, 1 done, < 0 error code */
+  uint32_t batch_size;                   /* requests in the batch it ran in */
+  char message[128];                     /* error message when status < 0 */
+} PropagServerResult;
+
+typedef struct propag_server propag_server;
+propag_server *propag_server_create(const PropagServerOptions *opt);
+/* Returns the request id (>= 0) or a negative status.  The buffers must stay
+ * valid until the request is done. */
+int64_t propag_server_submit(propag_server *server, const PropagJob *job,
+                             const PropagTerrainPtrs *terrain, uint64_t device_bytes);
+/* 1 done (or failed: see out->status), 0 not yet, < 0 unknown id. */
+int propag_server_poll(propag_server *server, int64_t id, PropagServerResult *out);
+/* As poll, waiting up to timeout_ms for the request to finish. */
+int propag_server_wait(propag_server *server, int64_t id, PropagServerResult *out,
+                       uint32_t timeout_ms);
+/* Forgets a finished request. */
+int propag_server_release(propag_server *server, int64_t id);
+/* Runs the queue dry, then frees the server. */
+void propag_server_destroy(propag_server *server);
+
 /* A batch captured as one CUDA graph: the fire pass of every job whose
  * terrain is given (terrains[i], device pointers; terrains may be NULL to
  * skip the fire pass, the jobs' fire rasters then being inputs), then the

@@ -554,6 +554,19 @@ static void to_stats(const StatsDev &h, PropagStats &o) {
   o.t_done_ns = h.t_done_ns;
 }
 
+extern "C" int propag_engine_last_stats(propag_engine *e, void *stream, PropagStats *stats,
+                                        uint32_t n_jobs) {
+  if (!e || !stats) return fail(PROPAG_ERR_INVALID, "null argument");
+  if (!e->last_stats) return fail(PROPAG_ERR_INVALID, "the engine has not run");
+  CK(cudaSetDevice(e->device));
+  std::vector<StatsDev> hs(n_jobs);
+  CK(cudaMemcpyAsync(hs.data(), e->last_stats, sizeof(StatsDev) * n_jobs, cudaMemcpyDeviceToHost,
+                     (cudaStream_t)stream));
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  for (uint32_t i = 0; i < n_jobs; ++i) to_stats(hs[i], stats[i]);
+  return PROPAG_OK;
+}
+
 extern "C" int propag_graph_stats(propag_graph *g, void *stream, PropagStats *stats) {
   if (!g || !stats) return fail(PROPAG_ERR_INVALID, "null argument");
   propag_engine *e = g->eng;

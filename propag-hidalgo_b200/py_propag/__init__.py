@@ -506,6 +506,66 @@ class Graph:
             pass
 
 
+class Server:
+    """Continuous-batching server (propag_server_*): submit device-resident
+    scenarios from any thread; a dispatcher batches what is waiting onto free
+    streams.  Results are dicts with the job's statistics, host times (ns)
+    and the batch size it ran in."""
+
+    def __init__(self, hbm_budget=0, lanes=0, max_batch=0, device=-1):
+        opt = L.PropagServerOptions(int(hbm_budget), int(lanes), int(max_batch), int(device), 0)
+        self._h = L.lib().propag_server_create(C.byref(opt))
+        if not self._h:
+            _raise(L.PROPAG_ERR_CUDA, "propag_server_create")
+
+    def submit(self, job, terrain=None, device_bytes=0) -> int:
+        rid = L.lib().propag_server_submit(self._h, C.byref(job),
+                                           C.byref(terrain) if terrain is not None else None,
+                                           int(device_bytes))
+        if rid < 0:
+            _raise(int(rid), "propag_server_submit")
+        return int(rid)
+
+    @staticmethod
+    def _result(r):
+        if r.status < 0:
+            raise PropagCudaError(f"request failed ({r.status}): {r.message.decode()}")
+        d = r.stats.as_dict()
+        d.update(submit_ns=int(r.submit_ns), start_ns=int(r.start_ns), done_ns=int(r.done_ns),
+                 batch_size=int(r.batch_size))
+        return d
+
+    def poll(self, rid):
+        r = L.PropagServerResult()
+        rc = L.lib().propag_server_poll(self._h, int(rid), C.byref(r))
+        if rc < 0:
+            _raise(rc, "propag_server_poll")
+        return self._result(r) if rc == 1 else None
+
+    def wait(self, rid, timeout_ms=600_000):
+        r = L.PropagServerResult()
+        rc = L.lib().propag_server_wait(self._h, int(rid), C.byref(r), int(timeout_ms))
+        if rc < 0:
+            _raise(rc, "propag_server_wait")
+        if rc == 0:
+            raise TimeoutError(f"request {rid} not done after {timeout_ms} ms")
+        return self._result(r)
+
+    def release(self, rid):
+        L.lib().propag_server_release(self._h, int(rid))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().propag_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def autotune(jobs, terrains=None, stream=0, repeats=1):
     """Fastest cluster size for this batch (propag_autotune): returns
     (options dict, milliseconds)."""
@@ -535,5 +595,5 @@ __all__ = [
     "PropagResults", "PyPropagResults", "propagate", "load_terrain_data", "check_cuda_available",
     "PropagCudaError", "PropagGdalError", "PropagValidationError", "PropagMPIError",
     "fire_behaviour", "propagate_arrays", "rasterize_ignitions", "write_geotiff", "point_wkb",
-    "demo_terrain", "Engine", "Graph", "autotune", "build",
+    "demo_terrain", "Engine", "Graph", "Server", "autotune", "build",
 ]

@@ -132,6 +132,17 @@ class PropagJob(C.Structure):
                 ("boundaries", C.c_void_p)]
 
 
+class PropagServerOptions(C.Structure):
+    _fields_ = [("hbm_budget", C.c_uint64), ("lanes", C.c_uint32), ("max_batch", C.c_uint32),
+                ("device", C.c_int32), ("pad", C.c_int32)]
+
+
+class PropagServerResult(C.Structure):
+    _fields_ = [("stats", PropagStats), ("submit_ns", C.c_uint64), ("start_ns", C.c_uint64),
+                ("done_ns", C.c_uint64), ("status", C.c_int32), ("batch_size", C.c_uint32),
+                ("message", C.c_char * 128)]
+
+
 # name -> (restype, argtypes); every symbol of both headers
 SIGNATURES = {
     "FFIPropagation_run": (C.c_bool, [FFIPropagation, C.c_size_t, C.c_char_p]),
@@ -163,6 +174,14 @@ SIGNATURES = {
     "propag_engine_run": (C.c_int, [C.c_void_p, C.POINTER(PropagJob), C.c_uint32, C.c_void_p,
                                     C.POINTER(PropagStats)]),
     "propag_engine_last_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float * 3)]),
+    "propag_engine_last_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PropagStats), C.c_uint32]),
+    "propag_server_create": (C.c_void_p, [C.POINTER(PropagServerOptions)]),
+    "propag_server_submit": (C.c_int64, [C.c_void_p, C.POINTER(PropagJob), C.POINTER(PropagTerrainPtrs),
+                                         C.c_uint64]),
+    "propag_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(PropagServerResult)]),
+    "propag_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(PropagServerResult), C.c_uint32]),
+    "propag_server_release": (C.c_int, [C.c_void_p, C.c_int64]),
+    "propag_server_destroy": (None, [C.c_void_p]),
     "propag_graph_create": (C.c_void_p, [C.POINTER(PropagOptions), C.POINTER(PropagJob),
                                          C.POINTER(PropagTerrainPtrs), C.c_uint32]),
     "propag_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
