@@ -275,6 +275,106 @@ def uneven_batch(L, dev, n):
     return _device_jobs(L, dev, items), desc
 
 
+def serve_leg(lib, L, pp, dev, master, seconds: float, rate: float, budget_gb: float,
+              check: int = 8) -> dict:
+    """Serving loop: Poisson arrivals of window requests cut from a
+    device-resident master terrain, submitted to a continuous-batching server
+    as they arrive; latency = submit to done (host clock).  A sample of the
+    requests is re-run alone through the plain path and compared bit for bit."""
+    import torch
+    from py_propag import scenarios as S
+    reqs = S.config4_requests(master["fuel_code"], seconds=seconds, rate=rate)
+    H, W = master["fuel_code"].shape
+    mt = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in master.items()}
+    prep = torch.cuda.Stream(dev)
+    srv = pp.Server(hbm_budget=int(budget_gb * 1e9), lanes=4, max_batch=64)
+    keep, res, sample = {}, {}, {}
+    check_ids = set(range(0, len(reqs), max(1, len(reqs) // check)))
+
+    def make(i, r):
+        n, x0, y0 = r["size"], r["x0"], r["y0"]
+        with torch.cuda.stream(prep):
+            t = {k: v[y0:y0 + n, x0:x0 + n].contiguous().view(-1) for k, v in mt.items()}
+            t["wind_speed"] = torch.full((n * n,), r["wind_speed"], dtype=torch.float32, device=dev)
+            t["wind_azimuth"] = torch.full((n * n,), r["wind_azimuth"], dtype=torch.float32, device=dev)
+            for k in ("d1hr", "d10hr", "d100hr"):
+                t[k] = t[k] + np.float32(r["dead_offset"])
+            (jobs, terrains, kp) = _device_jobs(L, dev, [(n, n, 5.0, 5.0, r["max_time"], 0,
+                                                         [r["ignition"]], t)])
+        prep.synchronize()
+        return jobs[0], terrains[0], kp
+
+    def collect(block=False):
+        for rid in list(keep):
+            out = srv.wait(rid, 600_000) if block else srv.poll(rid)
+            if out is not None:
+                res[rid] = out
+                if rid in check_ids:
+                    sample[rid] = keep[rid]
+                del keep[rid]
+                srv.release(rid)
+
+    t_start = time.perf_counter()
+    ids = []
+    for i, r in enumerate(reqs):
+        while time.perf_counter() - t_start < r["arrival"]:
+            collect()
+            time.sleep(0.0005)
+        job, terr, kp = make(i, r)
+        rid = srv.submit(job, terr)
+        ids.append(rid)
+        keep[rid] = (job, terr, kp, r)
+    collect(block=True)
+    lat = np.array([(res[r]["done_ns"] - res[r]["submit_ns"]) / 1e6 for r in ids])
+    span = (max(res[r]["done_ns"] for r in ids) - min(res[r]["submit_ns"] for r in ids)) / 1e9
+    # capacity: the same requests again, closed loop with 64 outstanding
+    check_ids.clear()
+    cap_ids = []
+    t_cap = time.perf_counter()
+    for i, r in enumerate(reqs):
+        while len(keep) >= 64:
+            collect()
+            time.sleep(0.0002)
+        job, terr, kp = make(i, r)
+        rid = srv.submit(job, terr)
+        cap_ids.append(rid)
+        keep[rid] = (job, terr, kp, r)
+    collect(block=True)
+    capacity = len(reqs) / (time.perf_counter() - t_cap)
+    cap_batch = float(np.mean([res[r]["batch_size"] for r in cap_ids]))
+    srv.close()
+    # the sample alone through the plain path
+    eng = lib.propag_engine_create(C.byref(L.PropagOptions(0, 0, 0, -1)))
+    sptr = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    same = True
+    for rid, (job, terr, kp, r) in sample.items():
+        served = kp[0][3].clone()
+        kp[0][3].fill_(-1.0)
+        if lib.propag_fire_simple_device(job.width * job.height, C.byref(terr), job.speed_max,
+                                         job.azimuth_max, job.eccentricity, sptr) or \
+                lib.propag_engine_run(eng, C.byref(job), 1, sptr, None):
+            raise RuntimeError(L.last_error())
+        torch.cuda.synchronize()
+        same &= bool(torch.equal(served, kp[0][3]))
+    lib.propag_engine_destroy(eng)
+    sizes = np.array([r["size"] for r in reqs])
+    return {
+        "workload": (f"config4: Poisson arrivals at {rate:g}/s for {seconds:g} s ({len(reqs)} requests), "
+                     f"windows {sizes.min()}..{sizes.max()} square from a device-resident "
+                     f"{W}x{H} master terrain, per-request wind/moisture/ignition, 1-12 h, "
+                     f"HBM budget {budget_gb:g} GB"),
+        "value": len(reqs) / span, "unit": UNIT, "offered_rate": rate,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max())},
+        "batch_size_mean": float(np.mean([res[r]["batch_size"] for r in ids])),
+        "capacity": {"value": capacity, "unit": UNIT, "batch_size_mean": cap_batch,
+                     "note": "same requests, closed loop with 64 outstanding (host wall clock, "
+                             "request preparation included)"},
+        "matches_plain_bitwise": same, "checked_alone": len(sample),
+        "server": "4 streams, continuous batching (requests admitted while earlier batches run)",
+    }
+
+
 def batched_leg(lib, L, pp, stream, batch, desc, steps, warmup, plain_jobs) -> dict:
     """All jobs of a batch in one persistent launch, captured as a CUDA graph
     with the cluster size the autotuner picks, against the plain path: each
@@ -362,6 +462,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ensemble", type=int, default=256, help="members of the ensemble leg (0 = skip)")
     ap.add_argument("--uneven", type=int, default=64, help="scenarios of the uneven leg (0 = skip)")
+    ap.add_argument("--serve-seconds", type=float, default=30.0,
+                    help="length of the serving leg's arrival stream (0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="serving arrivals per second")
     ap.add_argument("--plain-members", type=int, default=256,
                     help="ensemble members timed one by one on the plain path")
     args = ap.parse_args()
@@ -514,6 +617,9 @@ def bench_b200(args):
         line["batched_uneven"] = batched_leg(lib, L, pp, stream, batch, bdesc, args.steps,
                                              args.warmup, args.uneven)
         del batch
+    if args.serve_seconds > 0 and args.workload == "config1":
+        line["serving"] = serve_leg(lib, L, pp, dev, sc.terrain, args.serve_seconds, args.serve_rate,
+                                    150.0)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(sc, stats["evaluations"], os.cpu_count() or 1)
     if world > 1:

@@ -308,3 +308,35 @@ def config3(n: int = 64, seed: int = 3, min_size: int = 128, max_size: int = 204
         out.append(Scenario(size, size, cell, cell, float(rng.uniform(3600.0, 43200.0)), terrain,
                             ign, f"config3-{i}-{size}"))
     return out
+
+
+def config4_requests(master_fuel: np.ndarray, seconds: float = 300.0, rate: float = 20.0,
+                     seed: int = 4, min_size: int = 256, max_size: int = 4096):
+    """Serving workload: Poisson arrivals at `rate` per second for `seconds`;
+    each request is a square window, side log-uniform in [min_size, max_size],
+    cut from a master terrain/fuel atlas at a random offset, with its own wind
+    speed (lognormal, median 6 m/s, sigma 0.3), direction (225 +- 30 deg),
+    dead-moisture offset (+-0.02), one ignition over burnable cells of the
+    window and max_time U(1, 12) h.  Returns a list of dicts sorted by
+    arrival time (s)."""
+    rng = np.random.default_rng(seed)
+    H, W = master_fuel.shape
+    out, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > seconds:
+            break
+        n = int(round(math.exp(rng.uniform(math.log(min_size), math.log(max_size)))))
+        n = min(n, W, H)
+        x0 = int(rng.integers(0, W - n + 1))
+        y0 = int(rng.integers(0, H - n + 1))
+        win = master_fuel[y0:y0 + n, x0:x0 + n]
+        if not np.any(win):
+            continue
+        (ix, iy), = _burnable_cells(win, rng, 1)
+        out.append(dict(arrival=t, size=n, x0=x0, y0=y0,
+                        wind_speed=float(np.exp(np.log(6.0) + 0.3 * rng.standard_normal())),
+                        wind_azimuth=float(np.deg2rad((225.0 + rng.uniform(-30.0, 30.0) + 180.0) % 360.0)),
+                        dead_offset=float(rng.uniform(-0.02, 0.02)), ignition=(ix, iy, 0.0),
+                        max_time=float(rng.uniform(3600.0, 43200.0))))
+    return out
