@@ -70,6 +70,19 @@ def _rank_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(value: float, world: int, dev) -> float:
+    """The largest of every rank's value (all ranks call it at the same
+    point); the value itself on one rank.  `dev` is the device of the
+    reduction tensor: the GPU under NCCL, the CPU under gloo."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _workload(name: str):
     from py_propag import scenarios as S
     if name == "config1":
@@ -560,11 +573,7 @@ def bench_b200(args):
     t_all1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total_ms = t_all0.elapsed_time(t_all1)
-    if world > 1:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(t_all0.elapsed_time(t_all1), world, dev)
     step_ms = [a.elapsed_time(b) for a, b in ev_step]
     fire_ms = [a.elapsed_time(b) for a, b in ev_fire]
     prop_ms = [m[1] for m in eng_ms]
@@ -662,11 +671,7 @@ def e2e_leg(lib, L, pp, sc, args, world, dev, dev_time):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
     same = np.array_equal(out_t.numpy().view(np.uint32), dev_time.view(np.uint32))
     return {"value": world * args.steps / e2e_s, "unit": UNIT,
             "h2d_bytes_per_step": N * 37 + len(sc.ignitions) * 12,

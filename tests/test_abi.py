@@ -277,6 +277,10 @@ def test_device_entry_points_fail_without_gpu(lib, L, pp):
         pytest.skip("a GPU is present")
     assert lib.propag_engine_create(None) is None
     assert "no CUDA device" in L.last_error()
+    assert lib.propag_server_create(None) is None
+    assert "no CUDA device" in L.last_error()
+    with pytest.raises(pp.PropagCudaError):
+        pp.Server()
     t = pp.demo_terrain(4, 4)
     with pytest.raises(pp.PropagCudaError, match="no CUDA device"):
         pp.fire_behaviour(t)
