@@ -97,6 +97,33 @@ int propag_fire_simple_host(uint64_t n, const PropagTerrainPtrs *terrain, float 
 int propag_fire_full_host(uint64_t n, const PropagTerrainPtrs *terrain,
                           const PropagFireFields *out);
 
+/* Per-cell weather for the dmoist model: temperature (deg C), relative
+ * humidity (%) and cloud cover (%) hour-major [24][n] (hour h of cell i at
+ * h * n + i); daily precipitation (mm) of the last six days day-major [6][n]
+ * (day d = d days before the forecast). */
+typedef struct PropagWeatherPtrs {
+  const float *temperature;
+  const float *humidity;
+  const float *cloud_cover;
+  const float *precipitation;
+} PropagWeatherPtrs;
+
+/* Dead fuel moisture of n cells at one hour (0..23) of a day in `month`
+ * (1..12), the dmoist model of crates/dmoist/src/lib.rs:55-137 evaluated per
+ * cell: 1-h moisture from the hour's weather, shading by cloud cover,
+ * exposure and slope, and the precipitation of the last six days; 10-h and
+ * 100-h moisture interpolated from hours 6 and 15.  slope is rise/run,
+ * aspect radians (as in the terrain rasters), fuel the NFFL code.  Outputs are
+ * the model's percent values times `scale` (0.01 gives the fractions the fire
+ * pass takes).  Device pointers, stream-ordered. */
+int propag_dmoist_device(uint64_t n, int hour, int month, const PropagWeatherPtrs *weather,
+                         const float *slope, const float *aspect, const uint8_t *fuel,
+                         float scale, float *d1hr, float *d10hr, float *d100hr, void *stream);
+/* Same over host buffers (copies in and out, synchronises). */
+int propag_dmoist_host(uint64_t n, int hour, int month, const PropagWeatherPtrs *weather,
+                       const float *slope, const float *aspect, const uint8_t *fuel, float scale,
+                       float *d1hr, float *d10hr, float *d100hr);
+
 /* One ignited cell (the result of rasterising a TimeFeature). */
 typedef struct PropagIgnition {
   uint32_t x;

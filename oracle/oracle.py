@@ -211,6 +211,67 @@ def rounding_batch(x):
     return r, s
 
 
+# ---- dmoist (crates/dmoist/src/lib.rs) --------------------------------------
+
+_F, _I = C.c_float, C.c_int
+_DMOIST = {  # name -> (C function, argument types); float result
+    "hcb": ("odm_humidity_content_base", (_F, _F, _I), C.c_int),
+    "hcb_shading": ("odm_correct_hcb_for_shading", (_F, _F, _I, _F, _F, _I, _I), _F),
+    "prob_precip": ("odm_correct_probability_for_precipitation", (_F, _F), _F),
+    "d1hr": ("odm_d1hr", (_F, _F, _F), _F),
+    "x10hr": ("odm_moisture_by_10hr", (_I, _F, _F, _F), _F),
+    "live": ("odm_live_moisture", (_I,), _F),
+    "prob_ign": ("odm_ignition_probability", (_F, _F, _F, _I), _F),
+    "shading": ("odm_shading", (_F, _I), _F),
+    "wind_speed": ("odm_wind_speed", (C.c_double, C.c_double), C.c_double),
+    "wind_dir": ("odm_wind_direction", (C.c_double, C.c_double), C.c_double),
+}
+
+
+def dmoist_fn(name: str, params) -> np.ndarray:
+    """Evaluates one dmoist function row by row (params: rows x arguments)."""
+    lib = _load()
+    fname, argt, rest = _DMOIST[name]
+    fn = getattr(lib, fname)
+    fn.restype = rest
+    fn.argtypes = list(argt)
+    out = []
+    for row in np.asarray(params, dtype=np.float64):
+        args = [int(v) if t is _I else float(v) for v, t in zip(row, argt)]
+        out.append(float(fn(*args)))
+    return np.array(out)
+
+
+def dmoist_max_precip(month: int, pp) -> float:
+    lib = _load()
+    lib.odm_maximum_precipitation_effect.restype = C.c_float
+    a = np.ascontiguousarray(pp, dtype=np.float32)
+    return float(lib.odm_maximum_precipitation_effect(C.c_int(month), _ptr(a)))
+
+
+def dmoist_hourly(t, rh, cc, slope, aspect, pp, month, fuel):
+    """calculate_hourly_fuel_moisture for one site: (d1, d10, d100), 24 each."""
+    lib = _load()
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (t, rh, cc, pp)]
+    out = [np.zeros(24, np.float32) for _ in range(3)]
+    lib.odm_hourly(_ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), C.c_float(slope), C.c_float(aspect),
+                   _ptr(arrs[3]), C.c_int(month), C.c_int(fuel), *[_ptr(o) for o in out])
+    return tuple(out)
+
+
+def dmoist_cells(hour, month, t, rh, cc, slope, aspect, fuel, pp):
+    """Per-cell moisture at one hour: weather (24, n), precipitation (6, n)."""
+    lib = _load()
+    n = np.asarray(slope).size
+    t, rh, cc, pp = (np.ascontiguousarray(a, dtype=np.float32) for a in (t, rh, cc, pp))
+    slope, aspect = (np.ascontiguousarray(a, dtype=np.float32).ravel() for a in (slope, aspect))
+    fuel = np.ascontiguousarray(fuel, dtype=np.uint8).ravel()
+    out = [np.zeros(n, np.float32) for _ in range(3)]
+    lib.odm_cells(C.c_int64(n), C.c_int(hour), C.c_int(month), _ptr(t), _ptr(rh), _ptr(cc), _ptr(slope),
+                  _ptr(aspect), _ptr(fuel), _ptr(pp), *[_ptr(o) for o in out])
+    return tuple(out)
+
+
 def dda_cells(fx, fy, tx, ty):
     """Cells visited by the line-of-sight walk (propag.h:91-135)."""
     lib = _load()

@@ -869,6 +869,68 @@ extern "C" int propag_fire_full_host(uint64_t n, const PropagTerrainPtrs *terrai
   return fire_host(true, n, terrain, outs);
 }
 
+// ============================================================== dmoist ====
+namespace propag {
+cudaError_t launch_dmoist(uint64_t n, int hour, int month, const float *t, const float *rh,
+                          const float *cc, const float *pp, const float *slope, const float *aspect,
+                          const uint8_t *fuel, float scale, float *d1, float *d10, float *d100,
+                          int sm_count, cudaStream_t stream);
+}
+
+extern "C" int propag_dmoist_device(uint64_t n, int hour, int month, const PropagWeatherPtrs *w,
+                                    const float *slope, const float *aspect, const uint8_t *fuel,
+                                    float scale, float *d1hr, float *d10hr, float *d100hr,
+                                    void *stream) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (hour < 0 || hour > 23) return fail(PROPAG_ERR_INVALID, "hour must be 0..23");
+  if (!w || !w->temperature || !w->humidity || !w->cloud_cover || !w->precipitation || !slope ||
+      !aspect || !fuel || !d1hr || !d10hr || !d100hr)
+    return fail(PROPAG_ERR_INVALID, "null dmoist argument");
+  if (n == 0) return PROPAG_OK;
+  CK(launch_dmoist(n, hour, month, w->temperature, w->humidity, w->cloud_cover, w->precipitation, slope,
+                   aspect, fuel, scale, d1hr, d10hr, d100hr, sms, (cudaStream_t)stream));
+  return PROPAG_OK;
+}
+
+extern "C" int propag_dmoist_host(uint64_t n, int hour, int month, const PropagWeatherPtrs *w,
+                                  const float *slope, const float *aspect, const uint8_t *fuel,
+                                  float scale, float *d1hr, float *d10hr, float *d100hr) {
+  int rc = ensure_device(-1, nullptr);
+  if (rc) return rc;
+  if (!w || !w->temperature || !w->humidity || !w->cloud_cover || !w->precipitation || !slope ||
+      !aspect || !fuel || !d1hr || !d10hr || !d100hr)
+    return fail(PROPAG_ERR_INVALID, "null dmoist argument");
+  if (n == 0) return PROPAG_OK;
+  HostPath &hp = host_path();
+  std::lock_guard<std::mutex> lk(hp.mu);
+  cudaStream_t s = 0;
+  const size_t f4 = align_up(n * 4, 256), hw = align_up(24 * n * 4, 256), pw = align_up(6 * n * 4, 256);
+  CK(hp.buf.reserve(3 * hw + pw + 2 * f4 + align_up(n, 256) + 3 * f4, s));
+  size_t o = 0;
+  auto take = [&](size_t bytes) { char *p = hp.buf.at<char>(o); o += bytes; return p; };
+  float *t = (float *)take(hw), *rh = (float *)take(hw), *cc = (float *)take(hw), *pp = (float *)take(pw);
+  float *sl = (float *)take(f4), *as = (float *)take(f4);
+  uint8_t *fu = (uint8_t *)take(align_up(n, 256));
+  float *o1 = (float *)take(f4), *o10 = (float *)take(f4), *o100 = (float *)take(f4);
+  CK(cudaMemcpyAsync(t, w->temperature, 24 * n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(rh, w->humidity, 24 * n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(cc, w->cloud_cover, 24 * n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(pp, w->precipitation, 6 * n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(sl, slope, n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(as, aspect, n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(fu, fuel, n, cudaMemcpyHostToDevice, s));
+  PropagWeatherPtrs dw{t, rh, cc, pp};
+  rc = propag_dmoist_device(n, hour, month, &dw, sl, as, fu, scale, o1, o10, o100, s);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(d1hr, o1, n * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(d10hr, o10, n * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(d100hr, o100, n * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return PROPAG_OK;
+}
+
 // ======================================================= plain drop-in ====
 namespace {
 struct RunHostState {

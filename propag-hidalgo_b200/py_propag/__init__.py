@@ -434,6 +434,31 @@ def fire_behaviour(terrain: dict, full: bool = False) -> dict:
     return {k: v.reshape(shape) for k, v in out.items()}
 
 
+def dead_fuel_moisture(temperature, humidity, cloud_cover, precipitation, slope, aspect, fuel_code,
+                       hour: int, month: int, scale: float = 1.0) -> dict:
+    """Hourly dead fuel moisture per cell (the dmoist model) over host
+    arrays: weather (24, ...) per hour, precipitation (6, ...) per day, the
+    rest per cell.  Returns d1hr/d10hr/d100hr in the model's percent units
+    times ``scale`` (0.01 for the fractions fire_behaviour takes)."""
+    lib = L.lib()
+    shape = np.asarray(slope).shape
+    n = int(np.prod(shape))
+    w = [np.ascontiguousarray(a, dtype=np.float32).reshape(k, n)
+         for a, k in ((temperature, 24), (humidity, 24), (cloud_cover, 24), (precipitation, 6))]
+    sl, asp = (np.ascontiguousarray(a, dtype=np.float32).ravel() for a in (slope, aspect))
+    fu = np.ascontiguousarray(fuel_code, dtype=np.uint8).ravel()
+    if sl.size != n or asp.size != n or fu.size != n:
+        raise PropagValidationError("slope, aspect and fuel_code must have one value per cell")
+    ptrs = L.PropagWeatherPtrs(*[a.ctypes.data for a in w])
+    out = {k: np.empty(n, np.float32) for k in ("d1hr", "d10hr", "d100hr")}
+    rc = lib.propag_dmoist_host(n, int(hour), int(month), C.byref(ptrs), sl.ctypes.data, asp.ctypes.data,
+                                fu.ctypes.data, float(scale), out["d1hr"].ctypes.data,
+                                out["d10hr"].ctypes.data, out["d100hr"].ctypes.data)
+    if rc != 0:
+        _raise(rc, "dead_fuel_moisture")
+    return {k: v.reshape(shape) for k, v in out.items()}
+
+
 class Engine:
     """Batched propagation over device-resident scenarios (propag_engine_*).
     Jobs are ``PropagJob`` structures holding device pointers."""
@@ -595,5 +620,5 @@ __all__ = [
     "PropagResults", "PyPropagResults", "propagate", "load_terrain_data", "check_cuda_available",
     "PropagCudaError", "PropagGdalError", "PropagValidationError", "PropagMPIError",
     "fire_behaviour", "propagate_arrays", "rasterize_ignitions", "write_geotiff", "point_wkb",
-    "demo_terrain", "Engine", "Graph", "Server", "autotune", "build",
+    "demo_terrain", "Engine", "Graph", "Server", "autotune", "dead_fuel_moisture", "build",
 ]

@@ -132,6 +132,11 @@ class PropagJob(C.Structure):
                 ("boundaries", C.c_void_p)]
 
 
+class PropagWeatherPtrs(C.Structure):
+    _fields_ = [("temperature", C.c_void_p), ("humidity", C.c_void_p), ("cloud_cover", C.c_void_p),
+                ("precipitation", C.c_void_p)]
+
+
 class PropagServerOptions(C.Structure):
     _fields_ = [("hbm_budget", C.c_uint64), ("lanes", C.c_uint32), ("max_batch", C.c_uint32),
                 ("device", C.c_int32), ("pad", C.c_int32)]
@@ -174,6 +179,12 @@ SIGNATURES = {
     "propag_engine_run": (C.c_int, [C.c_void_p, C.POINTER(PropagJob), C.c_uint32, C.c_void_p,
                                     C.POINTER(PropagStats)]),
     "propag_engine_last_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float * 3)]),
+    "propag_dmoist_device": (C.c_int, [C.c_uint64, C.c_int, C.c_int, C.POINTER(PropagWeatherPtrs),
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    "propag_dmoist_host": (C.c_int, [C.c_uint64, C.c_int, C.c_int, C.POINTER(PropagWeatherPtrs),
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]),
     "propag_engine_last_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PropagStats), C.c_uint32]),
     "propag_server_create": (C.c_void_p, [C.POINTER(PropagServerOptions)]),
     "propag_server_submit": (C.c_int64, [C.c_void_p, C.POINTER(PropagJob), C.POINTER(PropagTerrainPtrs),
