@@ -97,6 +97,15 @@ int propag_fire_simple_host(uint64_t n, const PropagTerrainPtrs *terrain, float 
 int propag_fire_full_host(uint64_t n, const PropagTerrainPtrs *terrain,
                           const PropagFireFields *out);
 
+/* Slope (rise/run) and aspect (compass azimuth of the downhill direction,
+ * radians in [0, 2 pi), 0 on flat ground) from a DEM of width x height cells,
+ * for the terrain rasters.  Central differences inside the grid, one-sided on
+ * its edges, in double precision; dx and dy are the signed cell sizes of the
+ * geo transform (dy < 0 for north-up).  Device pointers, stream-ordered.  No
+ * counterpart in the reference, whose loader supplies slope and aspect. */
+int propag_slope_aspect_device(uint32_t width, uint32_t height, double dx, double dy,
+                               const float *dem, float *slope, float *aspect, void *stream);
+
 /* Per-cell weather for the dmoist model: temperature (deg C), relative
  * humidity (%) and cloud cover (%) hour-major [24][n] (hour h of cell i at
  * h * n + i); daily precipitation (mm) of the last six days day-major [6][n]

@@ -869,6 +869,26 @@ extern "C" int propag_fire_full_host(uint64_t n, const PropagTerrainPtrs *terrai
   return fire_host(true, n, terrain, outs);
 }
 
+// ================================================== terrain preparation ==
+namespace propag {
+cudaError_t launch_slope_aspect(int W, int H, double dx, double dy, const float *dem, float *slope,
+                                float *aspect, int sm_count, cudaStream_t stream);
+}
+
+extern "C" int propag_slope_aspect_device(uint32_t width, uint32_t height, double dx, double dy,
+                                          const float *dem, float *slope, float *aspect,
+                                          void *stream) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (!valid_size(width, height)) return fail(PROPAG_ERR_INVALID, "width/height must be 1..65534");
+  if (!(dx != 0.0) || !(dy != 0.0) || !std::isfinite(dx) || !std::isfinite(dy))
+    return fail(PROPAG_ERR_INVALID, "invalid pixel size");
+  if (!dem || !slope || !aspect) return fail(PROPAG_ERR_INVALID, "null raster");
+  CK(launch_slope_aspect((int)width, (int)height, dx, dy, dem, slope, aspect, sms, (cudaStream_t)stream));
+  return PROPAG_OK;
+}
+
 // ============================================================== dmoist ====
 namespace propag {
 cudaError_t launch_dmoist(uint64_t n, int hour, int month, const float *t, const float *rh,

@@ -185,8 +185,13 @@ bool write_geotiff_f32(const std::string &path, const GeoReference &g, const flo
   while (w.buf.size() & 3) w.buf.push_back(0);
   const size_t tiles_at = w.buf.size();
   for (uint32_t t = 0; t < nt; ++t) offsets[t] = (uint32_t)(tiles_at + (size_t)t * T * T * 4);
-  for (size_t i = 0; i < e.size(); ++i)
-    if (e[i].tag == 324) std::memcpy(w.buf.data() + payload_at[i], offsets.data(), nt * 4);
+  // the tile offsets: inline in the IFD entry when there is one tile (4 bytes),
+  // else in the entry's out-of-line payload
+  for (size_t i = 0; i < e.size(); ++i) {
+    if (e[i].tag != 324) continue;
+    std::memcpy(e[i].data.data(), offsets.data(), nt * 4);
+    if (e[i].data.size() > 4) std::memcpy(w.buf.data() + payload_at[i], offsets.data(), nt * 4);
+  }
   // IFD
   size_t at = ifd;
   auto put16 = [&](uint16_t v) { w.buf[at++] = v & 0xFF; w.buf[at++] = v >> 8; };

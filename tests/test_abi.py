@@ -308,11 +308,13 @@ def _read_tiff(path):
     return b, tags
 
 
-def test_geotiff_round_trip(pp, tmp_path):
-    w, h = 300, 270  # two tiles wide, two high, ragged edges
+@pytest.mark.parametrize("w,h", [(300, 270), (100, 80), (256, 256), (257, 1)])
+def test_geotiff_round_trip(pp, tmp_path, w, h):
+    """Several tiles with ragged edges, a single tile (its offset inline in
+    the IFD entry), exactly one full tile, a one-row grid."""
     g = pp.PyGeoReference(w, h, PROJ, [500000.0, 5.0, 0.0, 4000000.0, 0.0, -5.0])
     data = np.arange(w * h, dtype=np.float32).reshape(h, w) * 0.5
-    data[5, 7] = np.finfo(np.float32).max
+    data[min(5, h - 1), 7] = np.finfo(np.float32).max
     path = str(tmp_path / "t.tif")
     pp.write_geotiff(path, g, data)
     b, tags = _read_tiff(path)
@@ -323,14 +325,15 @@ def test_geotiff_round_trip(pp, tmp_path):
     assert mt[0] == 5.0 and mt[3] == 500000.0 and mt[5] == -5.0 and mt[7] == 4000000.0
     assert PROJ in tags[34737]
     offs = tags[324]
-    assert len(offs) == 4
+    tx, ty = (w + 255) // 256, (h + 255) // 256
+    assert len(offs) == tx * ty
     out = np.empty((h, w), np.float32)
     for t, off in enumerate(offs):
         tile = np.frombuffer(b, dtype="<f4", count=256 * 256, offset=off).reshape(256, 256)
-        r0, c0 = (t // 2) * 256, (t % 2) * 256
+        r0, c0 = (t // tx) * 256, (t % tx) * 256
         rr, cc = min(256, h - r0), min(256, w - c0)
         out[r0:r0 + rr, c0:c0 + cc] = tile[:rr, :cc]
         assert np.all(tile[rr:, :] == np.finfo(np.float32).max)
     assert np.array_equal(out, data)
     with pytest.raises(pp.PropagValidationError):
-        pp.write_geotiff(path, g, data[:10])
+        pp.write_geotiff(path, g, data.ravel()[:10])
