@@ -109,6 +109,7 @@ __device__ __forceinline__ float dot5(const float *c, const float m[5]) {
   return fmaf(c[4], m[4], s);
 }
 
+template <bool kFull>
 __device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], float ws,
                                           float waz, float slope, float aspect, FireOut &o) {
   // rx_int_rbqig
@@ -179,7 +180,7 @@ __device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], 
   o.speed_max = smax * kFpmToMps;
   o.azimuth_max = az;
   o.eccentricity = __fdiv_rn(sqrtf(a * (2.0f + a)), 1.0f + a);
-  {  // the remaining FireCuda fields, Byram and flame
+  if (kFull) {  // the remaining FireCuda fields, Byram and flame
     o.rx_int = rx * kRxToSI;
     o.speed0 = speed0 * kFpmToMps;
     o.hpua = rx * F.residence_time * kHpuaToSI;
@@ -208,81 +209,37 @@ __device__ __forceinline__ void store_cell(const Outputs &out, uint64_t i, const
     if (out.f[k]) out.f[k][i] = v[k];
 }
 
+template <bool kFull>
 __device__ __forceinline__ void one_cell(const FuelConst *cat, const Inputs &in, const Outputs &out,
                                          uint64_t i) {
-  const uint8_t code = in.fuel[i];
+  const uint8_t code = __ldg(in.fuel + i);
   FireOut o{};
   if (code < kMaxFuels && cat[code].has_fire != 0.0f) {
-    const float m[5] = {in.m[0][i], in.m[1][i], in.m[2][i], in.m[3][i], in.m[4][i]};
-    burn_cell(cat[code], m, in.ws[i], in.waz[i], in.slope[i], in.aspect[i], o);
+    const float m[5] = {__ldg(in.m[0] + i), __ldg(in.m[1] + i), __ldg(in.m[2] + i), __ldg(in.m[3] + i),
+                        __ldg(in.m[4] + i)};
+    burn_cell<kFull>(cat[code], m, __ldg(in.ws + i), __ldg(in.waz + i), __ldg(in.slope + i),
+                     __ldg(in.aspect + i), o);
   }
   store_cell(out, i, o);
 }
 
-// Vector path: all pointers 16-byte aligned; cells [0, n4*4) in groups of 4.
+// One cell per thread, grid-stride: every load and store is coalesced (4 or
+// 1 consecutive bytes per lane) and one copy of the cell code keeps the
+// kernel small in the instruction cache.  kFull: all ten fields; else the
+// three the propagation needs (the shared fields are the same operations,
+// so both give bit-identical values for them).
+template <bool kFull>
 __global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, uint64_t n) {
-  __shared__ FuelConst cat[kMaxFuels];
-  for (int t = threadIdx.x; t < (int)(sizeof(cat) / 4); t += blockDim.x)
-    reinterpret_cast<float *>(cat)[t] = reinterpret_cast<const float *>(c_catalog)[t];
-  __syncthreads();
-  const uint64_t n4 = n / 4;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n4; g += stride) {
-    const uchar4 fc = __ldg(reinterpret_cast<const uchar4 *>(in.fuel) + g);
-    float4 mv[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) mv[k] = __ldg(reinterpret_cast<const float4 *>(in.m[k]) + g);
-    const float4 ws = __ldg(reinterpret_cast<const float4 *>(in.ws) + g);
-    const float4 wa = __ldg(reinterpret_cast<const float4 *>(in.waz) + g);
-    const float4 sl = __ldg(reinterpret_cast<const float4 *>(in.slope) + g);
-    const float4 as = __ldg(reinterpret_cast<const float4 *>(in.aspect) + g);
-    const uint8_t codes[4] = {fc.x, fc.y, fc.z, fc.w};
-    FireOut o[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      o[c] = FireOut{};
-      const uint8_t code = codes[c];
-      if (code < kMaxFuels && cat[code].has_fire != 0.0f) {
-        const float m[5] = {(&mv[0].x)[c], (&mv[1].x)[c], (&mv[2].x)[c], (&mv[3].x)[c],
-                            (&mv[4].x)[c]};
-        burn_cell(cat[code], m, (&ws.x)[c], (&wa.x)[c], (&sl.x)[c], (&as.x)[c], o[c]);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 10; ++k) {
-      if (!out.f[k]) continue;
-      float4 v;
-      float *vp = &v.x;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const float vv[10] = {o[c].rx_int, o[c].speed0, o[c].hpua, o[c].phi_eff_wind,
-                              o[c].speed_max, o[c].azimuth_max, o[c].eccentricity,
-                              o[c].residence_time, o[c].byrams, o[c].flame};
-        vp[c] = vv[k];
-      }
-      reinterpret_cast<float4 *>(out.f[k])[g] = v;
-    }
-  }
-  // tail
-  const uint64_t t0 = n4 * 4;
-  for (uint64_t i = t0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-    one_cell(cat, in, out, i);
-}
-
-// Scalar path for unaligned pointers.
-__global__ void __launch_bounds__(256) fire_kernel_scalar(Inputs in, Outputs out, uint64_t n) {
   __shared__ FuelConst cat[kMaxFuels];
   for (int t = threadIdx.x; t < (int)(sizeof(cat) / 4); t += blockDim.x)
     reinterpret_cast<float *>(cat)[t] = reinterpret_cast<const float *>(c_catalog)[t];
   __syncthreads();
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-    one_cell(cat, in, out, i);
+    one_cell<kFull>(cat, in, out, i);
 }
 
 // ---- host-side launchers (called from api.cpp) ------------------------------
-static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
-
 cudaError_t upload_catalog() {
   FuelConst table[kMaxFuels];
   build_catalog_table(table);
@@ -295,25 +252,15 @@ cudaError_t launch_fire(bool full, uint64_t n, const uint8_t *fuel, const float 
                         cudaStream_t stream) {
   Inputs in{fuel, {m[0], m[1], m[2], m[3], m[4]}, ws, waz, slope, aspect};
   Outputs out{};
-  bool aligned = ((uintptr_t)fuel & 3u) == 0;
-  for (int k = 0; k < 5; ++k) aligned = aligned && aligned16(m[k]);
-  aligned = aligned && aligned16(ws) && aligned16(waz) && aligned16(slope) && aligned16(aspect);
-  for (int k = 0; k < 10; ++k) {
-    out.f[k] = outs[k];
-    if (outs[k]) aligned = aligned && aligned16(outs[k]);
-  }
+  for (int k = 0; k < 10; ++k) out.f[k] = outs[k];
   if (n == 0) return cudaSuccess;
   const int threads = 256;
-  const uint64_t work = aligned ? (n + 3) / 4 : n;
-  uint64_t blocks = (work + threads - 1) / threads;
+  uint64_t blocks = (n + threads - 1) / threads;
   const uint64_t cap = (uint64_t)sm_count * 8;  // 8 resident blocks per SM
   if (blocks > cap) blocks = cap;
   if (blocks == 0) blocks = 1;
-  // one compiled code path for every field selection: the 3-field and the
-  // 10-field calls give bit-identical values for the fields they share
-  (void)full;
-  if (aligned) fire_kernel<<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
-  else fire_kernel_scalar<<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
+  if (full) fire_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
+  else fire_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
   return cudaGetLastError();
 }
 
