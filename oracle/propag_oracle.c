@@ -81,7 +81,7 @@ static inline float sqrt_rz(float x) {
 /* ---- portable float cosine / arctangent ------------------------------------
  * cos: Cody-Waite reduction by pi/2 (three-part constant, fma), Taylor
  * polynomials on [-pi/4, pi/4].  atan2: octant reduction, atan(t) for
- * t in [0,1] with t > tan(pi/8) mapped through (t-1)/(t+1), Taylor series to
+ * t = mn/mx in [0,1], above tan(pi/8) as u = (mn-mx)/(mn+mx) (one division either way), Taylor series to
  * u^19.  Accuracy is checked against libm in the tests (<= 2 ulp). */
 static const float PIO2_HI = 1.57079637050628662109375f;
 static const float PIO2_MID = -4.37113900018624283e-8f;
@@ -126,12 +126,15 @@ float pg_atan2f(float y, float x) {
   float mx = ax > ay ? ax : ay;
   float mn = ax > ay ? ay : ax;
   if (mx == 0.0f) return 0.0f;
-  float t = mn / mx;
+  /* one division: t = mn / mx, or (t - 1) / (t + 1) formed directly as
+   * (mn - mx) / (mn + mx) above tan(pi/8) */
   float base = 0.0f;
-  float u = t;
-  if (t > TAN_PI_8) {
-    u = (t - 1.0f) / (t + 1.0f);
+  float u;
+  if (mn > TAN_PI_8 * mx) {
+    u = (mn - mx) / (mn + mx);
     base = PIO4_F;
+  } else {
+    u = mn / mx;
   }
   float u2 = u * u;
   float p = fmaf(u2, 5.26315789e-2f, -5.88235294e-2f); /*  1/19, -1/17 */

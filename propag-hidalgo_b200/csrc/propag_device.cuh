@@ -29,7 +29,7 @@ __device__ __forceinline__ int ref_y(uint32_t r) { return (int)(r >> 16); }
 // ---- portable float cosine / arctangent ------------------------------------
 // cos: Cody-Waite reduction by pi/2 with a three-part constant, Taylor
 // polynomials on [-pi/4, pi/4].  atan2: octant reduction; atan(t), t in [0,1],
-// with t > tan(pi/8) mapped through (t-1)/(t+1) and a Taylor series to u^19.
+// above tan(pi/8) as u = (mn-mx)/(mn+mx) (one division either way), Taylor to u^19.
 // Both are accurate to about 1 ulp and, being plain IEEE operations, give the
 // same bits on every IEEE machine.
 __device__ __forceinline__ float pg_sin_poly(float r) {
@@ -65,12 +65,15 @@ __device__ __forceinline__ float pg_atan2f(float y, float x) {
   const float mx = ax > ay ? ax : ay;
   const float mn = ax > ay ? ay : ax;
   if (mx == 0.0f) return 0.0f;
-  const float t = __fdiv_rn(mn, mx);
+  // one division: t = mn / mx, or (t - 1) / (t + 1) formed directly as
+  // (mn - mx) / (mn + mx) above tan(pi/8)
   float base = 0.0f;
-  float u = t;
-  if (t > 0.414213562373095049f) {
-    u = __fdiv_rn(__fsub_rn(t, 1.0f), __fadd_rn(t, 1.0f));
+  float u;
+  if (mn > __fmul_rn(0.414213562373095049f, mx)) {
+    u = __fdiv_rn(__fsub_rn(mn, mx), __fadd_rn(mn, mx));
     base = 0.785398163397448309616f;
+  } else {
+    u = __fdiv_rn(mn, mx);
   }
   const float u2 = __fmul_rn(u, u);
   float p = __fmaf_rn(u2, 5.26315789e-2f, -5.88235294e-2f);
