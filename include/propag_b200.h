@@ -140,10 +140,20 @@ typedef struct PropagIgnition {
   float time;
 } PropagIgnition;
 
+/* PropagOptions.cluster: group mode.  The engine's co-resident CTAs split
+ * into teams of at least 32 (one per scenario, up to that), launched
+ * cooperatively without clusters; a team keeps its tiles in global memory and
+ * meets at a counter barrier in global memory whose waits are bounded (a wait
+ * that gives up fails the run with PROPAG_ERR_TIMEOUT).  One scenario then
+ * runs on the whole device instead of one cluster.  Results are identical in
+ * every mode. */
+#define PROPAG_CLUSTER_GROUPS (-1)
+
 typedef struct PropagOptions {
   int32_t tile;    /* default super-grid tile side; 0 = PROPAG_DEFAULT_TILE,
                       PROPAG_TILE_WHOLE_GRID = one tile for the whole grid */
-  int32_t cluster; /* CTAs (one cluster) cooperating on one scenario, 1..16; 0 = auto */
+  int32_t cluster; /* CTAs (one cluster) cooperating on one scenario, 1..16; 0 = auto;
+                      PROPAG_CLUSTER_GROUPS = group mode (below) */
   int32_t threads; /* threads per CTA, multiple of 32, <= 512; 0 = 512 */
   int32_t device;  /* CUDA device ordinal; -1 = the current device */
 } PropagOptions;
@@ -166,6 +176,9 @@ typedef struct PropagStats {
   uint32_t max_walk;     /* longest line-of-sight walk (cells) */
   uint64_t t_start_ns;   /* device clock (ns) when a cluster took the job */
   uint64_t t_done_ns;    /* device clock (ns) when its propagation finished */
+  uint64_t scan_cells;   /* cells visited by referrer scans (sum of the scanned box areas) */
+  uint64_t cyc_wait;     /* SM cycles the team leader waited at phase barriers (included
+                            in the phase cycles above) */
 } PropagStats;
 
 /* One scenario of a batch.  All pointers are device pointers; time, refs and

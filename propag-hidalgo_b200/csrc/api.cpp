@@ -36,7 +36,7 @@ cudaError_t launch_ignite(const JobDev *jobs, uint32_t n_jobs, cudaStream_t stre
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
                           uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
                           StatsDev *stats, unsigned long long max_sweeps, const uint32_t *order,
-                          cudaStream_t stream);
+                          uint32_t group, cudaStream_t stream);
 cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n);
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
                         StatsDev *stats, cudaStream_t stream);
@@ -122,6 +122,10 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 bool valid_size(uint32_t w, uint32_t h) { return w >= 1 && h >= 1 && w <= 65534 && h <= 65534; }
 
+const char *status_text(uint32_t status) {
+  return status == kStatusGroupTimeout ? "a group barrier wait gave up" : "sweep limit reached";
+}
+
 }  // namespace
 }  // namespace propag
 
@@ -131,11 +135,12 @@ using namespace propag;
 struct propag_engine {
   int device = 0;
   int sms = 0;
-  int csize = 0;    // 0 = auto
+  int csize = 0;    // 0 = auto, PROPAG_CLUSTER_GROUPS = teams of CTAs without clusters
   int threads = 512;  // the engine kernel's launch bound
   int default_tile = PROPAG_DEFAULT_TILE;
   size_t smem_budget = 200 * 1024;  // dynamic shared memory per CTA for resident tiles
   int last_cluster = 0;             // cluster size and shared memory of the last run
+  uint32_t last_group = 0;          // CTAs per team of the last run (group mode), else 0
   size_t last_smem = 0;
   cudaStream_t stream = nullptr;  // the stream of the last run
   DevBuf job_scratch, slot_scratch, meta;
@@ -155,8 +160,8 @@ extern "C" propag_engine *propag_engine_create(const PropagOptions *opt) {
   cudaGetDevice(&e->device);
   e->sms = sms;
   if (opt) {
-    if (opt->cluster < 0 || opt->cluster > 16) {
-      fail(PROPAG_ERR_INVALID, "cluster must be 0..16");
+    if ((opt->cluster < 0 && opt->cluster != PROPAG_CLUSTER_GROUPS) || opt->cluster > 16) {
+      fail(PROPAG_ERR_INVALID, "cluster must be 0..16 or PROPAG_CLUSTER_GROUPS");
       delete e;
       return nullptr;
     }
@@ -300,29 +305,50 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     }
   }
   size_t smem = 0, tn_max = 1, ovf_cap = 0;
-  for (uint32_t i = 0; i < n_jobs; ++i) {
-    // exact referrer boxes when they fit, else the coarse ones
-    const bool exact = smem_bytes(tw[i], th[i], csize, true) <= budget;
-    jd[i].smem_tile = exact ? kSmemTileExact : fits(i, csize) ? kSmemTileCoarse : kSmemTileGlobal;
-    if (jd[i].smem_tile != kSmemTileGlobal) {
-      smem = std::max(smem, smem_bytes(tw[i], th[i], csize, exact));
-      ovf_cap = std::max<size_t>(ovf_cap, (size_t)smem_cap(tw[i], th[i], csize));
-    } else {
+  uint32_t n_slots = 0, group = 0;
+  if (csize == PROPAG_CLUSTER_GROUPS) {
+    // group mode: the co-resident CTAs split into teams of at least 32 CTAs
+    // (one team per job up to that), tiles in global memory
+    smem = global_tile_smem(e->threads);
+    int ctas = 0;
+    CK(engine_max_clusters(1, e->threads, smem, &ctas));
+    if (ctas < 2) return fail(PROPAG_ERR_CUDA, "group mode needs at least 2 resident CTAs");
+    n_slots = std::min<uint32_t>(n_jobs, (uint32_t)std::max(1, ctas / 32));
+    group = (uint32_t)ctas / n_slots;
+    for (uint32_t i = 0; i < n_jobs; ++i) {
+      jd[i].smem_tile = kSmemTileGlobal;
       tn_max = std::max<size_t>(tn_max, (size_t)tw[i] * (size_t)th[i]);
     }
+    csize = 1;
+  } else {
+    for (uint32_t i = 0; i < n_jobs; ++i) {
+      // exact referrer boxes when they fit, else the coarse ones
+      const bool exact = smem_bytes(tw[i], th[i], csize, true) <= budget;
+      jd[i].smem_tile = exact ? kSmemTileExact : fits(i, csize) ? kSmemTileCoarse : kSmemTileGlobal;
+      if (jd[i].smem_tile != kSmemTileGlobal) {
+        smem = std::max(smem, smem_bytes(tw[i], th[i], csize, exact));
+        ovf_cap = std::max<size_t>(ovf_cap, (size_t)smem_cap(tw[i], th[i], csize));
+      } else {
+        tn_max = std::max<size_t>(tn_max, (size_t)tw[i] * (size_t)th[i]);
+        smem = std::max(smem, global_tile_smem(e->threads));
+      }
+    }
+    int max_clusters = 0;
+    CK(engine_max_clusters(csize, e->threads, smem, &max_clusters));
+    if (max_clusters < 1) return fail(PROPAG_ERR_CUDA, "cluster size " + std::to_string(csize) + " cannot be resident");
+    n_slots = std::min<uint32_t>(n_jobs, (uint32_t)max_clusters);
   }
-  int max_clusters = 0;
-  CK(engine_max_clusters(csize, e->threads, smem, &max_clusters));
-  if (max_clusters < 1) return fail(PROPAG_ERR_CUDA, "cluster size " + std::to_string(csize) + " cannot be resident");
-  const uint32_t n_slots = std::min<uint32_t>(n_jobs, (uint32_t)max_clusters);
-  e->last_cluster = csize;
+  e->last_cluster = group ? PROPAG_CLUSTER_GROUPS : csize;
+  e->last_group = group;
   e->last_smem = smem;
   const size_t words_max = tn_max / 32 + 1;
+  // global-memory tiles: each CTA of a team has its own update region
+  const size_t team_ctas = group ? group : (size_t)csize;
+  const size_t upd_max = tn_max + 32 * (team_ctas + 1);
   const size_t ovf_list_bytes = align_up((size_t)csize * ovf_cap * 2, 256);
   const size_t ovf_upd_bytes = align_up((size_t)csize * ovf_cap * sizeof(Update), 256);
-  const size_t slot_bytes = align_up(tn_max * 4, 256) * 3 + align_up(words_max * 4, 256) +
-                            align_up(tn_max * sizeof(Update), 256) + 256 + ovf_list_bytes +
-                            ovf_upd_bytes;
+  const size_t slot_bytes = align_up(words_max * 4, 256) + align_up(upd_max * sizeof(Update), 256) +
+                            256 + ovf_list_bytes + ovf_upd_bytes;
   CK(e->slot_scratch.reserve(slot_bytes * n_slots, stream));
   // meta: jobs, slots, stats, queue
   const size_t meta_jobs = align_up(sizeof(JobDev) * n_jobs, 256);
@@ -357,16 +383,10 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   for (uint32_t s = 0; s < n_slots; ++s) {
     size_t o = slot_bytes * s;
     SlotDev &sd = e->slots_pinned[s];
-    sd.cand[0] = e->slot_scratch.at<uint32_t>(o);
-    o += align_up(tn_max * 4, 256);
-    sd.cand[1] = e->slot_scratch.at<uint32_t>(o);
-    o += align_up(tn_max * 4, 256);
-    sd.scan = e->slot_scratch.at<uint32_t>(o);
-    o += align_up(tn_max * 4, 256);
     sd.dirty = e->slot_scratch.at<uint32_t>(o);
     o += align_up(words_max * 4, 256);
     sd.upd = e->slot_scratch.at<Update>(o);
-    o += align_up(tn_max * sizeof(Update), 256);
+    o += align_up(upd_max * sizeof(Update), 256);
     sd.ctr = e->slot_scratch.at<uint32_t>(o);
     o += 256;
     sd.ovf_list = e->slot_scratch.at<uint16_t>(o);
@@ -376,7 +396,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     sd.pad = 0;
     // the dirty bitmap and counters must start cleared
     CK(cudaMemsetAsync(sd.dirty, 0, words_max * 4, stream));
-    CK(cudaMemsetAsync(sd.ctr, 0, 64, stream));
+    CK(cudaMemsetAsync(sd.ctr, 0, 64, stream));  // counters and barrier arrivals
   }
   JobDev *d_jobs = e->meta.at<JobDev>(0);
   SlotDev *d_slots = e->meta.at<SlotDev>(meta_jobs);
@@ -392,14 +412,14 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   const bool live = capturing == cudaStreamCaptureStatusNone;
   if (live) CK(cudaEventRecord(e->staged, stream));
   CK(cudaMemsetAsync(d_stats, 0, sizeof(StatsDev) * n_jobs, stream));
-  CK(cudaMemsetAsync(d_queue, 0, 4, stream));
+  CK(cudaMemsetAsync(d_queue, 0, 8, stream));  // queue position, group error flag
   // ---- kernels ----
   if (live) CK(cudaEventRecord(e->ev[0], stream));
   CK(launch_prep(d_jobs, n_jobs, max_cells, e->sms, stream));
   CK(launch_ignite(d_jobs, n_jobs, stream));
   if (live) CK(cudaEventRecord(e->ev[1], stream));
   CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, smem, d_queue, d_stats,
-                   1ull << 40, d_order, stream));
+                   1ull << 40, d_order, group, stream));
   if (live) CK(cudaEventRecord(e->ev[2], stream));
   CK(launch_post(d_jobs, n_jobs, max_cells, e->sms, d_stats, stream));
   if (live) CK(cudaEventRecord(e->ev[3], stream));
@@ -427,9 +447,11 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
       o.max_walk = hs[i].max_walk;
       o.t_start_ns = hs[i].t_start_ns;
       o.t_done_ns = hs[i].t_done_ns;
+      o.scan_cells = hs[i].scan_cells;
+      o.cyc_wait = hs[i].cyc_wait;
     }
     for (uint32_t i = 0; i < n_jobs; ++i)
-      if (hs[i].status) return fail(PROPAG_ERR_TIMEOUT, "job " + std::to_string(i) + ": sweep limit reached");
+      if (hs[i].status) return fail(PROPAG_ERR_TIMEOUT, "job " + std::to_string(i) + ": " + status_text(hs[i].status));
   }
   return PROPAG_OK;
 }
@@ -552,6 +574,8 @@ static void to_stats(const StatsDev &h, PropagStats &o) {
   o.max_walk = h.max_walk;
   o.t_start_ns = h.t_start_ns;
   o.t_done_ns = h.t_done_ns;
+  o.scan_cells = h.scan_cells;
+  o.cyc_wait = h.cyc_wait;
 }
 
 extern "C" int propag_engine_last_stats(propag_engine *e, void *stream, PropagStats *stats,
@@ -578,7 +602,7 @@ extern "C" int propag_graph_stats(propag_graph *g, void *stream, PropagStats *st
   CK(cudaStreamSynchronize((cudaStream_t)stream));
   for (uint32_t i = 0; i < g->n_jobs; ++i) to_stats(hs[i], stats[i]);
   for (uint32_t i = 0; i < g->n_jobs; ++i)
-    if (hs[i].status) return fail(PROPAG_ERR_TIMEOUT, "job " + std::to_string(i) + ": sweep limit reached");
+    if (hs[i].status) return fail(PROPAG_ERR_TIMEOUT, "job " + std::to_string(i) + ": " + status_text(hs[i].status));
   return PROPAG_OK;
 }
 
@@ -741,7 +765,7 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   CK(launch_prep(d_job, 1, N, sms, stream));
   CK(launch_ignite(d_job, 1, stream));
   CK(launch_engine(d_job, 1, d_slot, 1, csize, engine_threads(), smem, d_queue, d_stats, 1ull << 40,
-                   nullptr, stream));
+                   nullptr, 0u, stream));
   CK(launch_post(d_job, 1, N, sms, d_stats, stream));
   if (stats) {
     StatsDev h;
@@ -765,7 +789,9 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
     o.max_walk = h.max_walk;
     o.t_start_ns = h.t_start_ns;
     o.t_done_ns = h.t_done_ns;
-    if (h.status) return fail(PROPAG_ERR_TIMEOUT, "sweep limit reached");
+    o.scan_cells = h.scan_cells;
+    o.cyc_wait = h.cyc_wait;
+    if (h.status) return fail(PROPAG_ERR_TIMEOUT, status_text(h.status));
   }
   return PROPAG_OK;
 }

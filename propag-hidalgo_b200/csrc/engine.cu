@@ -159,7 +159,7 @@ __device__ __forceinline__ void dir_consts(const JobDev &j, DirConst &d) {
 
 struct Counters {
   uint32_t dda = 0, gat = 0, walk_max = 0;
-  unsigned long long evals = 0, scans = 0;
+  unsigned long long evals = 0, scans = 0, scan_cells = 0;
 };
 
 // find_neighbor_which_reaches_first (propag.cu:124-190) evaluated by the 8
@@ -323,6 +323,7 @@ __device__ __forceinline__ void warp_scan_boxes(ScanBox *sb, const Box &box, uin
                                                 MarkFn mark_fn) {
   const uint32_t area = box.area();
   cnt.scans += area ? 1 : 0;
+  cnt.scan_cells += area;
   const uint32_t incl = warp_incl_scan(area, lane);
   const uint32_t total = __shfl_sync(kFull, incl, 31);
   if (total == 0) return;
@@ -359,6 +360,66 @@ __device__ __forceinline__ void sync_cluster() {
   cg::this_cluster().sync();
 }
 
+// ---- team synchronisation ----
+// The CTAs that work on one job meet at every phase boundary: at the hardware
+// cluster barrier, or in group mode (G CTAs of a cooperative launch without
+// clusters, tiles in global memory) at an arrival counter in global memory.
+// A group wait is bounded: when the other CTAs have not all arrived after
+// kGroupWaitNs, or once any CTA of the launch has given up, it sets the
+// launch's error flag and returns false, and the caller abandons the launch.
+constexpr unsigned long long kGroupWaitNs = 2000000000ull;  // 2 s; a phase takes < 50 ms
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+struct Team {
+  unsigned long long *bar;  // group mode: arrivals at the group's barriers; null = cluster
+  uint32_t *err;            // group mode: the launch's error flag
+  int *ok;                  // shared: this CTA's outcome of the last wait
+  uint32_t G;               // CTAs in the group
+  unsigned long long target = 0;
+  unsigned long long waited = 0;  // thread 0: cycles from arrival to release
+  // global_fence = false: cluster mode orders shared-memory accesses only
+  __device__ bool sync(bool global_fence = true) {
+    const long long t0 = threadIdx.x == 0 ? clock64() : 0;
+    if (!bar) {
+      if (global_fence) __threadfence();
+      cg::this_cluster().sync();
+      if (threadIdx.x == 0) waited += (unsigned long long)(clock64() - t0);
+      return true;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      target += G;  // every CTA of the group passes the same barriers
+      __threadfence();
+      atomicAdd(bar, 1ull);
+      bool good = true;
+      const unsigned long long start_ns = globaltimer_ns();
+      while (ld_acquire_u64(bar) < target) {
+        if (ld_relaxed_u32(err) != 0u || globaltimer_ns() - start_ns > kGroupWaitNs) {
+          good = false;
+          break;
+        }
+        __nanosleep(32);
+      }
+      if (!good) atomicOr(err, 1u);
+      __threadfence();
+      *ok = good ? 1 : 0;
+      waited += (unsigned long long)(clock64() - t0);
+    }
+    __syncthreads();
+    return *ok != 0;
+  }
+};
+
 // Referrer box update for a cell (x, y) that adopted reference r, in the
 // global arrays (fire-and-forget reductions).
 __device__ __forceinline__ void box_expand_global(const JobDev &j, uint32_t r, int x, int y) {
@@ -374,29 +435,25 @@ struct TileDesc {
 };
 
 // ================================================ global-memory tiles ====
-// Marks the 3x3 neighbourhood of tile cell (lx, ly) for the next sweep
-// (deduplicated through the dirty bitmap) and appends the new cells to work
-// list q.  Called by every lane of a warp; `active` selects the lanes.
-__device__ __forceinline__ void mark3x3_list(const SlotDev &s, int q, bool active, int lx, int ly,
-                                             int TW, int TH, uint32_t lane) {
-  uint32_t fresh = 0;
-  if (active) {
-#pragma unroll
-    for (int t = 0; t < 9; ++t) {
-      const int ax = lx + t % 3 - 1, ay = ly + t / 3 - 1;
-      if (t == 4 || ax < 0 || ay < 0 || ax >= TW || ay >= TH) continue;
-      const uint32_t k = (uint32_t)ax + (uint32_t)ay * (uint32_t)TW;
-      const uint32_t bit = 1u << (k & 31);
-      if (!(atomicOr(s.dirty + (k >> 5), bit) & bit)) fresh |= 1u << t;
-    }
-  }
-  uint32_t at = warp_append(s.ctr + q, __popc(fresh), lane);
+// The tile's state stays in global memory (L2).  The cells are dealt to the
+// team's R CTAs by 32-cell words of the tile's dirty bitmap, word w to CTA
+// w % R.  In the evaluate phase a CTA compacts the marked cells of its words
+// (all its cells on the first sweep) into a work list in shared memory, a
+// chunk of blockDim.x words at a time, evaluates them and appends its
+// improvements to its own region of the slot's update array; in the commit
+// phase it commits those improvements itself.  Marks for the next sweep set
+// bits in the bitmap with reductions (no return value), so the only global
+// atomic a sweep needs per CTA is the improvement count that ends the launch.
+
+// Marks the 3x3 neighbourhood of tile cell (lx, ly), centre excluded, in the
+// dirty bitmap.
+__device__ __forceinline__ void mark3x3_bits(uint32_t *dirty, int lx, int ly, int TW, int TH) {
 #pragma unroll
   for (int t = 0; t < 9; ++t) {
-    if (fresh & (1u << t)) {
-      const int ax = lx + t % 3 - 1, ay = ly + t / 3 - 1;
-      s.cand[q][at++] = (uint32_t)ax + (uint32_t)ay * (uint32_t)TW;
-    }
+    const int ax = lx + t % 3 - 1, ay = ly + t / 3 - 1;
+    if (t == 4 || ax < 0 || ay < 0 || ax >= TW || ay >= TH) continue;
+    const uint32_t k = (uint32_t)ax + (uint32_t)ay * (uint32_t)TW;
+    atomicOr(dirty + (k >> 5), 1u << (k & 31));
   }
 }
 
@@ -407,6 +464,7 @@ struct SweepCtx {
   unsigned long long cyc[4] = {0, 0, 0, 0};  // first sweeps, evaluate, commit, staging
   long long t_phase = 0;
   bool abort = false;
+  bool failed = false;  // a group wait gave up (implies abort)
   __device__ __forceinline__ void tick(int phase) {
     if (leader) {
       const long long now = clock64();
@@ -416,80 +474,113 @@ struct SweepCtx {
   }
 };
 
-// One tile launch with the state in global memory.  Returns whether any
-// sweep improved a cell.
+// One tile launch with the state in global memory, by a team of R CTAs
+// (this one is `rank`).  `list` is shared memory for blockDim.x * 32 u16
+// entries, `cta_ctr` two shared counters.  Returns whether any sweep
+// improved a cell.
 __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &s, const TileDesc &td,
-                            ScanBox *scan_boxes, uint32_t tid, uint32_t nthreads, SweepCtx &cx) {
-  const uint32_t lane = threadIdx.x & 31, gwarp = tid >> 5;
+                            ScanBox *scan_boxes, uint16_t *list, uint32_t *cta_ctr, uint32_t rank,
+                            uint32_t R, SweepCtx &cx, Team &team) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int x0 = td.x0, y0 = td.y0, TW = td.TW, TH = td.TH;
   const uint32_t TN = (uint32_t)TW * (uint32_t)TH;
+  const uint32_t nwords = (TN + 31) / 32;
+  const uint32_t mine = nwords > rank ? (nwords - rank + R - 1) / R : 0u;  // words of this CTA
+  Update *const upd = s.upd + (size_t)rank * global_tile_upd_cap(TN, R);
   bool first = true, worked = false;
   int p = 0;
   for (;;) {
-    // ---- evaluate (Jacobi: nothing is written to the state) ----
-    const uint32_t nitems = first ? TN : __ldcg(s.ctr + p);
     ++cx.sweeps;  // every thread counts, so the abort below is uniform
-    if (cx.leader) {
-      s.ctr[p ^ 1] = 0;
-      cx.cnt.evals += nitems;
-    }
-    // four cells per warp, eight lanes per cell
-    for (uint32_t base = gwarp * 4; base < nitems; base += (nthreads >> 5) * 4) {
-      const uint32_t ci = base + (lane >> 3);
-      const bool valid = ci < nitems;
-      uint32_t k = ci;
-      int x = 0, y = 0;
-      Best own{FLT_MAX, kNoRef};
-      if (valid) {
-        if (!first) {
-          k = __ldcg(s.cand[p] + ci);
-          if ((lane & 7) == 0) atomicAnd(s.dirty + (k >> 5), ~(1u << (k & 31)));
+    // ---- evaluate (Jacobi: nothing is written to the state) ----
+    if (threadIdx.x == 0) cta_ctr[1] = 0;
+    for (uint32_t c0 = 0; c0 < mine; c0 += blockDim.x) {
+      __syncthreads();  // the previous chunk's list is consumed
+      if (threadIdx.x == 0) cta_ctr[0] = 0;
+      __syncthreads();
+      const uint32_t t = c0 + threadIdx.x;  // this CTA's t-th word
+      uint32_t bits = 0;
+      if (t < mine) {
+        const uint32_t w = rank + t * R;
+        if (first) {
+          bits = (w == nwords - 1 && (TN & 31)) ? (1u << (TN & 31)) - 1u : 0xFFFFFFFFu;
+        } else {
+          bits = __ldcg(s.dirty + w);
+          if (bits) s.dirty[w] = 0u;
         }
-        x = x0 + (int)(k % (uint32_t)TW);
-        y = y0 + (int)(k / (uint32_t)TW);
-        const int64_t c = x + (int64_t)y * j.W;
-        own = Best{__ldcg(j.time + c), __ldcg(j.refs + c)};
       }
-      const Best b = evaluate_coop(j, dc, GlobalAcc{j}, x, y, own, valid, lane, cx.cnt);
-      const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
-      const uint32_t at = warp_append(s.ctr + 2, improved ? 1u : 0u, lane);
-      if (improved) s.upd[at] = Update{k, b.time, b.ref, 0u};
+      uint32_t at = warp_append(cta_ctr + 0, __popc(bits), lane);
+      for (; bits; bits &= bits - 1) list[at++] = (uint16_t)(threadIdx.x * 32 + __ffs(bits) - 1);
+      __syncthreads();
+      const uint32_t nlist = cta_ctr[0];
+      if (threadIdx.x == 0) cx.cnt.evals += nlist;
+      // four cells per warp, eight lanes per cell
+      for (uint32_t base = warp * 4; base < nlist; base += nwarps * 4) {
+        const uint32_t ci = base + (lane >> 3);
+        const bool valid = ci < nlist;
+        uint32_t k = 0;
+        int x = 0, y = 0;
+        Best own{FLT_MAX, kNoRef};
+        if (valid) {
+          const uint32_t e = list[ci];
+          k = (rank + (c0 + (e >> 5)) * R) * 32 + (e & 31);
+          x = x0 + (int)(k % (uint32_t)TW);
+          y = y0 + (int)(k / (uint32_t)TW);
+          const int64_t c = x + (int64_t)y * j.W;
+          own = Best{__ldcg(j.time + c), __ldcg(j.refs + c)};
+        }
+        const Best b = evaluate_coop(j, dc, GlobalAcc{j}, x, y, own, valid, lane, cx.cnt);
+        const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
+        const uint32_t ai = warp_append(cta_ctr + 1, improved ? 1u : 0u, lane);
+        if (improved) upd[ai] = Update{k, b.time, b.ref, 0u};
+      }
     }
-    sync_cluster();
+    __syncthreads();
+    const uint32_t my_upd = cta_ctr[1];
+    if (threadIdx.x == 0 && my_upd) atomicAdd(s.ctr + 2 + p, my_upd);
+    if (!team.sync()) {
+      cx.failed = cx.abort = true;
+      break;
+    }
     cx.tick(first ? 0 : 1);
-    const uint32_t nupd = __ldcg(s.ctr + 2);
+    const uint32_t nupd = __ldcg(s.ctr + 2 + p);
+    // the other parity's count, last read before the previous commit
+    // barrier, is cleared for the next sweep (also when this launch ends, so
+    // that the next tile launch finds both at zero)
+    if (cx.leader) s.ctr[2 + (p ^ 1)] = 0;
     if (nupd == 0) break;
     worked = true;
     // ---- commit (update_point / commit_point), mark, referrer scans ----
     // A referrer scan may run while other cells of this sweep commit: a cell
     // whose reference changes in this sweep is itself marked, and a box only
     // grows, so what the scan must find (referrers from earlier sweeps) is
-    // unaffected by the concurrent writes.
-    for (uint32_t base = gwarp * 32; base < nupd; base += nthreads) {
+    // unaffected by the concurrent writes.  Updates are dealt `per` to a
+    // warp, as few as spreads them over the CTA's warps (a warp's referrer
+    // scans run one after another).
+    const uint32_t per = min(32u, (my_upd + nwarps - 1) / nwarps);
+    for (uint32_t base = warp * per; base < my_upd; base += nwarps * per) {
       const uint32_t u = base + lane;
-      const bool valid = u < nupd;
+      const bool valid = lane < per && u < my_upd;
       int lx = 0, ly = 0;
       uint32_t want = 0;
-      bool burning = false;
       Box box{1, 1, 0, 0};
       if (valid) {
-        const Update up = s.upd[u];
-        lx = (int)(up.k % (uint32_t)TW);
-        ly = (int)(up.k / (uint32_t)TW);
+        const uint4 raw = __ldcg(reinterpret_cast<const uint4 *>(upd) + u);  // Update{k, time, ref}
+        const float ut = __uint_as_float(raw.y);
+        lx = (int)(raw.x % (uint32_t)TW);
+        ly = (int)(raw.x / (uint32_t)TW);
         const int x = x0 + lx, y = y0 + ly;
         const int64_t c = x + (int64_t)y * j.W;
-        j.time[c] = up.time;
-        j.refs[c] = up.ref;
+        j.time[c] = ut;
+        j.refs[c] = raw.z;
+        box_expand_global(j, raw.z, x, y);
         // only a burning cell is read by its neighbours
-        burning = up.time < j.max_time && __ldg(j.speed + c) != 0.0f;
-        box_expand_global(j, up.ref, x, y);
+        if (ut < j.max_time && __ldg(j.speed + c) != 0.0f) mark3x3_bits(s.dirty, lx, ly, TW, TH);
         want = pack_ref(x, y);
         const uint32_t bx0 = __ldcg(j.box_x0 + c);
         if (bx0 != kEmptyBox)
           box = clip_box((int)bx0, (int)__ldcg(j.box_y0 + c), (int)__ldcg(j.box_x1 + c),
                          (int)__ldcg(j.box_y1 + c), x0, y0, TW, TH, j.W, j.H);
       }
-      mark3x3_list(s, p ^ 1, burning, lx, ly, TW, TH, lane);
       warp_scan_boxes(
           scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cx.cnt,
           [&](int xx, int yy, float &t) {
@@ -498,15 +589,15 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
             return __ldcg(j.refs + n);
           },
           [&](bool hit, int xx, int yy) {
-            if (__any_sync(kFull, hit)) mark3x3_list(s, p ^ 1, hit, xx - x0, yy - y0, TW, TH, lane);
+            if (hit) mark3x3_bits(s.dirty, xx - x0, yy - y0, TW, TH);
           });
     }
-    sync_cluster();
-    cx.tick(2);
-    if (cx.leader) {
-      cx.improvements += nupd;
-      s.ctr[2] = 0;  // the update list was consumed
+    if (!team.sync()) {
+      cx.failed = cx.abort = true;
+      break;
     }
+    cx.tick(2);
+    if (cx.leader) cx.improvements += nupd;
     p ^= 1;
     first = false;
     if (cx.sweeps > cx.max_sweeps) {
@@ -721,7 +812,7 @@ struct SmemAcc {
 // referrer-box codec.
 template <class B>
 __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const SlotDev &slot,
-                          const TileDesc &td, ScanBox *scan_boxes, SweepCtx &cx) {
+                          const TileDesc &td, ScanBox *scan_boxes, SweepCtx &cx, Team &team) {
   using BoxT = typename B::T;
   cg::cluster_group cluster = cg::this_cluster();
   SmemGeom g;
@@ -772,7 +863,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
     sm.grown[w] = 0u;
   }
   if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = sm.ctr[2] = sm.ctr[3] = 0u;
-  cluster.sync();
+  team.sync(false);
   cx.tick(3);
 
   bool first = true, worked = false;
@@ -821,7 +912,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
     }
     __syncthreads();
     if (threadIdx.x == 0 && sm.ctr[1]) atomicAdd(rank_ptr(sm.ctr, 0) + 2 + par, sm.ctr[1]);
-    cluster.sync();
+    team.sync(false);
     cx.tick(first ? 0 : 1);
     const uint32_t total = rank_ptr(sm.ctr, 0)[2 + par];
     if (total == 0) break;
@@ -833,9 +924,12 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
       cx.improvements += total;
     }
     const uint32_t nupd = sm.ctr[1];
-    for (uint32_t base = threadIdx.x & ~31u; base < nupd; base += blockDim.x) {
+    // updates dealt `per` to a warp (see tile_global)
+    const uint32_t nwarps = blockDim.x >> 5;
+    const uint32_t per = min(32u, (nupd + nwarps - 1) / nwarps);
+    for (uint32_t base = (threadIdx.x >> 5) * per; base < nupd; base += nwarps * per) {
       const uint32_t u = base + lane;
-      const bool valid = u < nupd;
+      const bool valid = lane < per && u < nupd;
       uint32_t want = 0;
       Box box{1, 1, 0, 0};
       if (valid) {
@@ -889,7 +983,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
     }
     __syncthreads();
     if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = 0u;
-    cluster.sync();
+    team.sync(false);
     cx.tick(2);
     par ^= 1;
     first = false;
@@ -922,38 +1016,50 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
     }
   }
   if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = 0u;
-  sync_cluster();
+  team.sync();
   cx.tick(3);
   return worked;
 }
 
 // ================================================================ engine ====
+// Cluster mode (group == 0): every cluster is one team.  Group mode
+// (group = G > 1, launched cooperatively without clusters): CTAs
+// [g * G, (g + 1) * G) form team g, which keeps its tiles in global memory
+// and meets at the bounded counter barrier of its slot.
 __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev *__restrict__ jobs,
                                                          uint32_t n_jobs,
                                                          const SlotDev *__restrict__ slots,
                                                          uint32_t *__restrict__ queue,
                                                          StatsDev *__restrict__ stats,
                                                          unsigned long long max_sweeps,
-                                                         const uint32_t *__restrict__ order) {
+                                                         const uint32_t *__restrict__ order,
+                                                         uint32_t group) {
   extern __shared__ __align__(16) char dyn_smem[];
   cg::cluster_group cluster = cg::this_cluster();
-  const uint32_t csize = cluster.num_blocks();
+  const bool grouped = group > 1;
+  const uint32_t csize = grouped ? group : cluster.num_blocks();
   const uint32_t slot_id = blockIdx.x / csize;
   const SlotDev s = slots[slot_id];
-  const uint32_t nthreads = csize * blockDim.x;
-  const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
+  const uint32_t rank = grouped ? blockIdx.x % csize : cluster.block_rank();
+  const uint32_t tid = rank * blockDim.x + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   __shared__ DirConst dc;
   __shared__ JobDev js;
   __shared__ ScanBox scan_boxes[kEngineThreads];
+  __shared__ int team_ok;
+  __shared__ uint32_t cta_ctr[2];  // global-memory tiles: work list and update counts
+  Team team{grouped ? reinterpret_cast<unsigned long long *>(s.ctr + 8) : nullptr, queue + 1,
+            &team_ok, csize};
+  uint32_t taken = 0xFFFFFFFFu;  // tid 0: the queue position it took last
 
   for (;;) {
     if (tid == 0) {
-      s.ctr[4] = atomicAdd(queue, 1u);
+      taken = atomicAdd(queue, 1u);
+      s.ctr[4] = taken;
       s.ctr[0] = s.ctr[1] = s.ctr[2] = s.ctr[3] = 0;
     }
-    sync_cluster();
-    // clusters take the jobs in queue order; `order` (when given) maps queue
+    if (!team.sync()) break;
+    // teams take the jobs in queue order; `order` (when given) maps queue
     // positions to jobs, e.g. largest first so that the longest jobs start early
     const uint32_t q = __ldcg(s.ctr + 4);
     if (q >= n_jobs) return;
@@ -982,28 +1088,32 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
         td.TW = min(j.T, j.W - td.x0);
         td.TH = min(j.T, j.H - td.y0);
         const bool w = j.smem_tile == kSmemTileExact
-                           ? tile_smem<BoxExact>(j, dc, dyn_smem, s, td, scan_boxes, cx)
+                           ? tile_smem<BoxExact>(j, dc, dyn_smem, s, td, scan_boxes, cx, team)
                        : j.smem_tile == kSmemTileCoarse
-                           ? tile_smem<BoxCoarse>(j, dc, dyn_smem, s, td, scan_boxes, cx)
-                                   : tile_global(j, dc, s, td, scan_boxes, tid, nthreads, cx);
+                           ? tile_smem<BoxCoarse>(j, dc, dyn_smem, s, td, scan_boxes, cx, team)
+                           : tile_global(j, dc, s, td, scan_boxes,
+                                         reinterpret_cast<uint16_t *>(dyn_smem), cta_ctr, rank,
+                                         csize, cx, team);
         round_worked |= w;
       }
       if (!round_worked || cx.abort) break;
     }
     // per-job statistics
     Counters &cnt = cx.cnt;
-    unsigned long long evals = cnt.evals, scans = cnt.scans;
+    unsigned long long evals = cnt.evals, scans = cnt.scans, scan_cells = cnt.scan_cells;
     for (int o = 16; o > 0; o >>= 1) {
       cnt.dda += __shfl_xor_sync(kFull, cnt.dda, o);
       cnt.gat += __shfl_xor_sync(kFull, cnt.gat, o);
       cnt.walk_max = max(cnt.walk_max, __shfl_xor_sync(kFull, cnt.walk_max, o));
       scans += __shfl_xor_sync(kFull, scans, o);
+      scan_cells += __shfl_xor_sync(kFull, scan_cells, o);
       evals += __shfl_xor_sync(kFull, evals, o);
     }
     if (lane == 0) {
       if (cnt.dda) atomicAdd(&st->dda_steps, (unsigned long long)cnt.dda);
       if (cnt.gat) atomicAdd(&st->gathers, (unsigned long long)cnt.gat);
       if (scans) atomicAdd(&st->refbox_scans, scans);
+      if (scan_cells) atomicAdd(&st->scan_cells, scan_cells);
       if (evals) atomicAdd(&st->evaluations, evals);
       if (cnt.walk_max) atomicMax(&st->max_walk, cnt.walk_max);
     }
@@ -1016,10 +1126,17 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
       st->cyc_eval = cx.cyc[1];
       st->cyc_commit = cx.cyc[2];
       st->cyc_stage = cx.cyc[3];
-      if (cx.abort) st->status = kStatusSweepLimit;
+      if (cx.abort) st->status = cx.failed ? kStatusGroupTimeout : kStatusSweepLimit;
       st->t_done_ns = globaltimer_ns();
+      st->cyc_wait = team.waited;
     }
-    sync_cluster();
+    if (cx.failed || !team.sync()) break;
+  }
+  // A group wait gave up: this team's job and every job no team has taken
+  // yet are reported failed (the other teams stop at their next wait).
+  if (tid == 0) {
+    for (uint32_t q = taken; q < n_jobs; q = atomicAdd(queue, 1u))
+      stats[order ? __ldg(order + q) : q].status = kStatusGroupTimeout;
   }
 }
 
@@ -1098,15 +1215,32 @@ cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n) {
   return cudaOccupancyMaxActiveClusters(n, engine_kernel, &cfg);
 }
 
+// group == 0: n_slots clusters of csize CTAs.  group > 1: n_slots teams of
+// `group` CTAs in one cooperative launch (all CTAs co-resident, which the
+// teams' barriers need; the launch fails rather than run otherwise).
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
                           uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
                           StatsDev *stats, unsigned long long max_sweeps, const uint32_t *order,
-                          cudaStream_t stream) {
+                          uint32_t group, cudaStream_t stream) {
   cudaError_t e = engine_attrs(smem);
   if (e != cudaSuccess) return e;
   cudaLaunchAttribute attr[1];
+  if (group > 1) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_slots * group, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps,
+                              order, group);
+  }
   cudaLaunchConfig_t cfg = engine_config(csize, threads, n_slots * (unsigned)csize, smem, attr, stream);
-  return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps, order);
+  return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps, order,
+                            0u);
 }
 
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,

@@ -33,23 +33,37 @@ struct Update {
   uint32_t ref;
   uint32_t pad;
 };
+static_assert(sizeof(Update) == 16, "an update is read back as one 16-byte load");
 
-// Global-memory scratch of one cluster slot.  cand/dirty/scan/upd serve tile
-// launches that do not fit in shared memory (capacity = largest such tile
-// area of the batch); ovf_list/ovf_upd take the work-list and update-list
+// Global-memory scratch of one team slot.  dirty/upd serve tile launches
+// whose state stays in global memory: the tile's dirty bitmap and the
+// update array, CTA r of the team using entries from r * cap on (cap =
+// global_tile_upd_cap); ovf_list/ovf_upd take the work-list and update-list
 // entries of shared-memory tiles beyond their shared-memory capacity
 // (ovf_cap entries per CTA of the cluster, CTA r at offset r * ovf_cap).
 struct SlotDev {
-  uint32_t *cand[2];
   uint32_t *dirty;
-  uint32_t *scan;
   Update *upd;
-  uint32_t *ctr;  // [0..1] ncand, [2] nupd, [3] nscan, [4] job
+  // [0..1] unused, [2..3] update counts (by sweep parity), [4] job,
+  // [8..9] group-mode barrier arrivals (64-bit)
+  uint32_t *ctr;
   uint16_t *ovf_list;
   Update *ovf_upd;
   uint32_t ovf_cap;
   uint32_t pad;
 };
+
+// Update-array entries a CTA of an R-CTA team may need in one sweep of a
+// global-memory tile of TN cells (the cells of its bitmap words); the team
+// needs R times that, at most TN + 32 R.
+__host__ __device__ inline uint32_t global_tile_upd_cap(uint32_t TN, uint32_t R) {
+  const uint32_t nwords = (TN + 31) / 32;
+  return (nwords + R - 1) / R * 32;
+}
+
+// Shared memory a CTA needs for a global-memory tile launch: the u16 work
+// list of one chunk (32 cells of each of blockDim.x words).
+__host__ __device__ inline size_t global_tile_smem(int threads) { return (size_t)threads * 32 * 2; }
 
 // Per-job statistics accumulated on the device (PropagStats order).
 struct StatsDev {
@@ -62,9 +76,12 @@ struct StatsDev {
   // device clock (%globaltimer, ns) when a cluster took the job and when its
   // propagation finished
   unsigned long long t_start_ns, t_done_ns;
+  unsigned long long scan_cells, cyc_wait;
 };
 
 constexpr uint32_t kStatusSweepLimit = 1;
+// a group barrier wait gave up (group mode); the job's results are invalid
+constexpr uint32_t kStatusGroupTimeout = 2;
 
 // Shared-memory tile layout: rows of the tile plus its one-cell halo are
 // dealt to the cluster's CTAs round-robin (row hy -> CTA hy % C), so that a

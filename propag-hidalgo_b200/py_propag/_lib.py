@@ -20,6 +20,7 @@ PROPAG_ERR_TIMEOUT = -4
 PROPAG_ERR_OOM = -5
 PROPAG_DEFAULT_TILE = 323
 PROPAG_TILE_WHOLE_GRID = -1
+PROPAG_CLUSTER_GROUPS = -1  # PropagOptions.cluster: teams of CTAs over the whole device
 
 
 class GT(C.Structure):
@@ -117,10 +118,13 @@ class PropagStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in STAT_FIELDS] + [("status", C.c_uint32),
                                                          ("max_walk", C.c_uint32),
                                                          ("t_start_ns", C.c_uint64),
-                                                         ("t_done_ns", C.c_uint64)]
+                                                         ("t_done_ns", C.c_uint64),
+                                                         ("scan_cells", C.c_uint64),
+                                                         ("cyc_wait", C.c_uint64)]
 
     def as_dict(self):
-        return {k: int(getattr(self, k)) for k in STAT_FIELDS + ("status", "max_walk", "t_start_ns", "t_done_ns")}
+        return {k: int(getattr(self, k)) for k in STAT_FIELDS + ("status", "max_walk", "t_start_ns", "t_done_ns",
+                                                                   "scan_cells", "cyc_wait")}
 
 
 class PropagJob(C.Structure):

@@ -73,11 +73,12 @@ def test_ridges_lakes_roads_many_ignitions(pp, oracle, tile):
     assert res.stats["improvements"] > 0
 
 
-@pytest.mark.parametrize("cluster", [1, 2, 16])
+@pytest.mark.parametrize("cluster", [1, 2, 16, -1])
 def test_shared_memory_and_global_tiles(pp, oracle, cluster):
     """The same scenario with the tile resident in the cluster's shared
     memory (when it fits) and in global memory (cluster 1 cannot hold a
-    130 x 130 halo'd tile): both bit-exact against the restatement."""
+    130 x 130 halo'd tile; group mode, -1, always uses global memory): all
+    bit-exact against the restatement."""
     from py_propag import scenarios as S
     sc = S.config1(size=128, seed=5, n_ign=4, max_time=10000.0)
     s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
@@ -91,7 +92,7 @@ def test_shared_memory_and_global_tiles(pp, oracle, cluster):
         assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
 
 
-@pytest.mark.parametrize("tile,cluster", [(300, 16), (300, 8), (323, 0)])
+@pytest.mark.parametrize("tile,cluster", [(300, 16), (300, 8), (323, 0), (300, -1), (64, -1)])
 def test_wide_tiles_several_launches(pp, oracle, tile, cluster):
     """Tiles wider than 254 cells keep their staged referrer boxes at
     two-cell granularity; over several tile launches and rounds the scans
@@ -179,10 +180,10 @@ def _device_scenario(pp, sc):
     return dev
 
 
-@pytest.mark.parametrize("cluster", [1, 4, 16])
+@pytest.mark.parametrize("cluster", [1, 4, 16, -1])
 def test_batch_equals_single_runs(pp, oracle, cluster):
     """Uneven scenarios in one persistent launch give each scenario's own
-    result, whatever the cluster size."""
+    result, whatever the cluster size (-1: group mode, four teams)."""
     import torch
     from py_propag import _lib as L
     from py_propag import scenarios as S
