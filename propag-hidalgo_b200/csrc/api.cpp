@@ -136,6 +136,7 @@ struct propag_engine {
   int device = 0;
   int sms = 0;
   int csize = 0;    // 0 = auto, PROPAG_CLUSTER_GROUPS = teams of CTAs without clusters
+  bool auto_groups = true;  // auto may choose group mode (needs the whole device)
   int threads = 512;  // the engine kernel's launch bound
   int default_tile = PROPAG_DEFAULT_TILE;
   size_t smem_budget = 200 * 1024;  // dynamic shared memory per CTA for resident tiles
@@ -151,6 +152,13 @@ struct propag_engine {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around prep, engine, post
   StatsDev *last_stats = nullptr;  // device statistics of the last run's jobs
 };
+
+namespace propag {
+// Engines whose runs overlap other engines' runs on the device (the server's
+// lanes) keep to clusters: a group-mode launch is cooperative and occupies
+// every SM, so its teams would wait for CTAs that other kernels hold.
+void engine_keep_to_clusters(propag_engine *e) { e->auto_groups = false; }
+}  // namespace propag
 
 extern "C" propag_engine *propag_engine_create(const PropagOptions *opt) {
   int sms = 0;
@@ -274,6 +282,18 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   const size_t budget = e->smem_budget;
   auto fits = [&](uint32_t i, int c) { return smem_bytes(tw[i], th[i], c) <= budget; };
   int csize = e->csize;
+  if (csize == 0) {
+    // A few scenarios run fastest in group mode: one runs on one cluster at
+    // most (its tiles go one after another), so a cluster leaves most SMs idle,
+    // while teams of 37-148 CTAs spread each sweep over the whole device.
+    // Measured on B200 (1024^2 ensemble members): 1 scenario 79 ms in group
+    // mode against 120 ms on a 16-CTA cluster, 8 scenarios 162 against
+    // 194 ms; from 16 scenarios on, clusters are faster.
+    int ctas = 0;
+    CK(engine_max_clusters(1, e->threads, global_tile_smem(e->threads), &ctas));
+    if (e->auto_groups && ctas >= 64 && n_jobs <= (uint32_t)(2 * std::max(1, ctas / 32)))
+      csize = PROPAG_CLUSTER_GROUPS;
+  }
   if (csize == 0) {
     // among the cluster sizes that hold every job's tile, the one that runs
     // the most jobs at once (resident clusters, up to the job count); ties go
@@ -629,6 +649,7 @@ extern "C" int propag_autotune(const PropagJob *jobs, const PropagTerrainPtrs *t
     if (all) cands.push_back(c);
   }
   if (cands.empty()) cands.push_back(16);  // global-memory tiles: the largest cluster
+  cands.push_back(PROPAG_CLUSTER_GROUPS);
   cudaEvent_t a = nullptr, b = nullptr;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));

@@ -29,6 +29,11 @@
 
 #include "propag_b200.h"
 
+namespace propag {
+void engine_keep_to_clusters(propag_engine *e);  // api.cpp
+}
+using propag::engine_keep_to_clusters;
+
 namespace {
 
 uint64_t now_ns() {
@@ -182,6 +187,7 @@ extern "C" propag_server *propag_server_create(const PropagServerOptions *opt) {
   for (uint32_t i = 0; i < n_lanes; ++i) {
     Lane lane;
     lane.eng = propag_engine_create(&eo);  // selects the device, fails loudly without one
+    if (lane.eng) engine_keep_to_clusters(lane.eng);  // lanes run side by side
     if (!lane.eng ||
         cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&lane.done, cudaEventDisableTiming) != cudaSuccess) {

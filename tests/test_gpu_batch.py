@@ -47,13 +47,17 @@ def _uneven(n=6, seed=41):
     return S.config3(n=n, seed=seed, min_size=48, max_size=360)
 
 
-def test_graph_replays_equal_single_runs(pp):
+@pytest.mark.parametrize("cluster", [0, 16, -1])
+def test_graph_replays_equal_single_runs(pp, cluster):
+    """Six uneven scenarios captured once and replayed twice, with the
+    automatic choice (group mode for this few), 16-CTA clusters and group
+    mode (a cooperative launch inside the graph)."""
     import torch
     from py_propag import _lib as L
     scs = _uneven()
     tiles = [0 if i % 3 else 57 for i in range(len(scs))]
     jobs, terrains, keep = _device_batch(pp, L, scs, tiles)
-    g = pp.Graph(jobs, terrains)
+    g = pp.Graph(jobs, terrains, cluster=cluster)
     alone = [_alone(pp, sc, t) for sc, t in zip(scs, tiles)]
     for rep in range(2):
         for b in keep:
@@ -99,7 +103,7 @@ def test_autotune_picks_a_fitting_cluster_and_results_do_not_change(pp):
     tiles = [0] * len(scs)
     jobs, terrains, keep = _device_batch(pp, L, scs, tiles)
     opts, ms = pp.autotune(jobs, terrains, repeats=1)
-    assert opts["cluster"] in (1, 2, 4, 8, 16) and ms > 0
+    assert opts["cluster"] in (1, 2, 4, 8, 16, -1) and ms > 0
     g = pp.Graph(jobs, terrains, cluster=opts["cluster"])
     g.launch()
     torch.cuda.synchronize()
