@@ -149,6 +149,14 @@ typedef struct PropagIgnition {
  * every mode. */
 #define PROPAG_CLUSTER_GROUPS (-1)
 
+/* Self-test of group mode's bounded wait (no reference counterpart): runs an
+ * 8 x 8 scenario in group mode whose team counts one CTA more than the launch
+ * holds, so that its first barrier never completes.  Every CTA gives up after
+ * the wait limit (2 s); the call returns PROPAG_ERR_TIMEOUT with *status = 2
+ * (the job's device status: a group wait gave up), and the device stays
+ * usable. */
+int propag_selftest_group_wait(uint32_t *status);
+
 typedef struct PropagOptions {
   int32_t tile;    /* default super-grid tile side; 0 = PROPAG_DEFAULT_TILE,
                       PROPAG_TILE_WHOLE_GRID = one tile for the whole grid */

@@ -36,7 +36,7 @@ cudaError_t launch_ignite(const JobDev *jobs, uint32_t n_jobs, cudaStream_t stre
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
                           uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
                           StatsDev *stats, unsigned long long max_sweeps, const uint32_t *order,
-                          uint32_t group, cudaStream_t stream);
+                          uint32_t group, uint32_t phantom, cudaStream_t stream);
 cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n);
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
                         StatsDev *stats, cudaStream_t stream);
@@ -137,6 +137,7 @@ struct propag_engine {
   int sms = 0;
   int csize = 0;    // 0 = auto, PROPAG_CLUSTER_GROUPS = teams of CTAs without clusters
   bool auto_groups = true;  // auto may choose group mode (needs the whole device)
+  uint32_t phantom = 0;     // self-test only: CTAs a group-mode team waits for in vain
   int threads = 512;  // the engine kernel's launch bound
   int default_tile = PROPAG_DEFAULT_TILE;
   size_t smem_budget = 200 * 1024;  // dynamic shared memory per CTA for resident tiles
@@ -439,7 +440,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   CK(launch_ignite(d_jobs, n_jobs, stream));
   if (live) CK(cudaEventRecord(e->ev[1], stream));
   CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, smem, d_queue, d_stats,
-                   1ull << 40, d_order, group, stream));
+                   1ull << 40, d_order, group, group ? e->phantom : 0u, stream));
   if (live) CK(cudaEventRecord(e->ev[2], stream));
   CK(launch_post(d_jobs, n_jobs, max_cells, e->sms, d_stats, stream));
   if (live) CK(cudaEventRecord(e->ev[3], stream));
@@ -479,6 +480,40 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
 extern "C" int propag_engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs,
                                  void *stream, PropagStats *stats) {
   return engine_run(e, jobs, n_jobs, (cudaStream_t)stream, stats);
+}
+
+extern "C" int propag_selftest_group_wait(uint32_t *status) {
+  if (!status) return fail(PROPAG_ERR_INVALID, "null status");
+  *status = 0;
+  PropagOptions o{0, PROPAG_CLUSTER_GROUPS, 0, -1};
+  propag_engine *e = propag_engine_create(&o);
+  if (!e) return PROPAG_ERR_CUDA;  // message set by propag_engine_create
+  e->phantom = 1;
+  const uint32_t W = 8, H = 8, N = W * H;
+  DevBuf buf;
+  int rc = PROPAG_OK;
+  if (buf.reserve(N * 4 * 4 + N * 2 * 2 + 256, nullptr) != cudaSuccess ||
+      cudaMemset(buf.at<char>(0), 0, N * 4 * 4 + N * 2 * 2 + 256) != cudaSuccess) {
+    rc = fail(PROPAG_ERR_CUDA, "self-test buffers");
+  } else {
+    PropagJob j{};
+    j.width = W;
+    j.height = H;
+    j.dx = 5.0;
+    j.dy = 5.0;
+    j.max_time = 100.0f;
+    j.speed_max = buf.at<float>(0);
+    j.azimuth_max = buf.at<float>(N * 4);
+    j.eccentricity = buf.at<float>(N * 8);
+    j.time = buf.at<float>(N * 12);
+    j.refs_x = buf.at<uint16_t>(N * 16);
+    j.refs_y = buf.at<uint16_t>(N * 18);
+    PropagStats st{};
+    rc = engine_run(e, &j, 1, nullptr, &st);
+    *status = st.status;
+  }
+  propag_engine_destroy(e);
+  return rc;
 }
 
 extern "C" int propag_engine_last_times(propag_engine *e, float ms[3]) {
@@ -786,7 +821,7 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   CK(launch_prep(d_job, 1, N, sms, stream));
   CK(launch_ignite(d_job, 1, stream));
   CK(launch_engine(d_job, 1, d_slot, 1, csize, engine_threads(), smem, d_queue, d_stats, 1ull << 40,
-                   nullptr, 0u, stream));
+                   nullptr, 0u, 0u, stream));
   CK(launch_post(d_job, 1, N, sms, d_stats, stream));
   if (stats) {
     StatsDev h;

@@ -1218,10 +1218,12 @@ cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n) {
 // group == 0: n_slots clusters of csize CTAs.  group > 1: n_slots teams of
 // `group` CTAs in one cooperative launch (all CTAs co-resident, which the
 // teams' barriers need; the launch fails rather than run otherwise).
+// phantom > 0 (self-test of the bounded wait, one slot only): the team counts
+// `phantom` CTAs more than the launch holds, so its barriers never complete.
 cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *slots,
                           uint32_t n_slots, int csize, int threads, size_t smem, uint32_t *queue,
                           StatsDev *stats, unsigned long long max_sweeps, const uint32_t *order,
-                          uint32_t group, cudaStream_t stream) {
+                          uint32_t group, uint32_t phantom, cudaStream_t stream) {
   cudaError_t e = engine_attrs(smem);
   if (e != cudaSuccess) return e;
   cudaLaunchAttribute attr[1];
@@ -1235,8 +1237,9 @@ cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *sl
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (phantom && n_slots != 1) return cudaErrorInvalidValue;
     return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps,
-                              order, group);
+                              order, group + phantom);
   }
   cudaLaunchConfig_t cfg = engine_config(csize, threads, n_slots * (unsigned)csize, smem, attr, stream);
   return cudaLaunchKernelEx(&cfg, engine_kernel, jobs, n_jobs, slots, queue, stats, max_sweeps, order,

@@ -183,6 +183,7 @@ SIGNATURES = {
     "propag_engine_run": (C.c_int, [C.c_void_p, C.POINTER(PropagJob), C.c_uint32, C.c_void_p,
                                     C.POINTER(PropagStats)]),
     "propag_engine_last_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float * 3)]),
+    "propag_selftest_group_wait": (C.c_int, [C.POINTER(C.c_uint32)]),
     "propag_slope_aspect_device": (C.c_int, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "propag_dmoist_device": (C.c_int, [C.c_uint64, C.c_int, C.c_int, C.POINTER(PropagWeatherPtrs),

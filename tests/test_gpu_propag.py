@@ -218,3 +218,28 @@ def test_repeated_calls_are_deterministic(pp):
     keys = ("rounds", "launches", "sweeps", "evaluations", "improvements", "dda_steps", "gathers",
             "burned")
     assert {k: a.stats[k] for k in keys} == {k: b.stats[k] for k in keys}
+
+
+def test_group_wait_gives_up_and_device_stays_usable(pp, oracle):
+    """Group mode's team barrier is a bounded wait: a team that counts one
+    CTA more than its launch holds gives up after the limit, the call fails
+    with PROPAG_ERR_TIMEOUT and the job reports status 2; afterwards the
+    device runs group mode normally (bit-exact)."""
+    import time
+    from py_propag import _lib as L
+    from py_propag import scenarios as S
+    st = C.c_uint32(0)
+    t0 = time.perf_counter()
+    rc = L.lib().propag_selftest_group_wait(C.byref(st))
+    dt = time.perf_counter() - t0
+    assert rc == L.PROPAG_ERR_TIMEOUT, L.last_error()
+    assert st.value == 2
+    assert "group barrier" in L.last_error()
+    assert 1.5 < dt < 30.0
+    sc = S.config0(size=96, seed=3)
+    s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
+    res = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=0, cluster=-1)
+    sp, az, ec = _fire(pp, sc.terrain)
+    o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                         sc.ignitions, tile=0)
+    assert np.array_equal(res.arrival_times.view(np.uint32), o.time.view(np.uint32))
