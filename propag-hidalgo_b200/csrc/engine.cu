@@ -446,14 +446,26 @@ struct TileDesc {
 // atomic a sweep needs per CTA is the improvement count that ends the launch.
 
 // Marks the 3x3 neighbourhood of tile cell (lx, ly), centre excluded, in the
-// dirty bitmap.
+// dirty bitmap: per row the (up to) three cells are consecutive bits, so a
+// row takes one reduction, two where it straddles a word.
 __device__ __forceinline__ void mark3x3_bits(uint32_t *dirty, int lx, int ly, int TW, int TH) {
+  const int xa = max(lx - 1, 0), xb = min(lx + 1, TW - 1);  // columns of the 3x3 inside the tile
+  if (xa > xb) return;
 #pragma unroll
-  for (int t = 0; t < 9; ++t) {
-    const int ax = lx + t % 3 - 1, ay = ly + t / 3 - 1;
-    if (t == 4 || ax < 0 || ay < 0 || ax >= TW || ay >= TH) continue;
-    const uint32_t k = (uint32_t)ax + (uint32_t)ay * (uint32_t)TW;
-    atomicOr(dirty + (k >> 5), 1u << (k & 31));
+  for (int dy = -1; dy <= 1; ++dy) {
+    const int ay = ly + dy;
+    if (ay < 0 || ay >= TH) continue;
+    const uint32_t k0 = (uint32_t)xa + (uint32_t)ay * (uint32_t)TW;
+    // bits of columns xa..xb, without the centre on the middle row
+    uint32_t run = (1u << (xb - xa + 1)) - 1u;
+    if (dy == 0 && lx >= xa && lx <= xb) run &= ~(1u << (lx - xa));
+    const uint32_t w = k0 >> 5, b = k0 & 31;
+    const uint32_t lo = run << b;
+    if (lo) atomicOr(dirty + w, lo);
+    if (b + (uint32_t)(xb - xa) >= 32) {
+      const uint32_t hi = run >> (32 - b);
+      if (hi) atomicOr(dirty + w + 1, hi);
+    }
   }
 }
 
