@@ -242,7 +242,7 @@ int propag_engine_last_stats(propag_engine *engine, void *stream, PropagStats *s
  * first and writes the job's fire rasters).  Whenever a lane is free the
  * dispatcher takes the requests waiting at that moment, up to max_batch and
  * within hbm_budget bytes of device memory in flight (each request counts
- * `device_bytes`, 64 B per cell when 0), and runs them as one batch on that
+ * `device_bytes`, 96 B per cell when 0), and runs them as one batch on that
  * lane; requests that arrive while batches are on the GPU are admitted as
  * lanes and memory free up, and run alongside them.  A request's results are
  * the same alone and in any batch.  No counterpart in the reference (one

@@ -258,7 +258,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     tw[i] = std::min<int>(T, (int)j.width);
     th[i] = std::min<int>(T, (int)j.height);
     off[i] = job_bytes;
-    job_bytes += align_up(N * 4, 256) * 5 + (j.boundaries ? 0 : align_up(words * 4, 256));
+    // references, referrer boxes, boundary bits, 8 travel-time planes
+    job_bytes += align_up(N * 4, 256) * 13 + (j.boundaries ? 0 : align_up(words * 4, 256));
     max_cells = std::max<uint64_t>(max_cells, N);
   }
   CK(e->job_scratch.reserve(job_bytes, stream));
@@ -276,6 +277,9 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     jd[i].box_x1 = arr[3];
     jd[i].box_y1 = arr[4];
     jd[i].bnd = jobs[i].boundaries ? jobs[i].boundaries : e->job_scratch.at<uint32_t>(o);
+    if (!jobs[i].boundaries) o += align_up(((N + 31) / 32) * 4, 256);
+    jd[i].tt = e->job_scratch.at<float>(o);
+    jd[i].tt_plane = (int64_t)(align_up(N * 4, 256) / 4);
   }
   // ---- cluster size and tile residency ----
   // A tile launch runs in the cluster's shared memory when the tile and its

@@ -60,11 +60,43 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
+// Per-scenario constants of the eight neighbour directions, in the
+// reference's neighbour order (j outer, i inner, centre skipped): the bearing
+// from the neighbour to the cell and their distance, computed with the same
+// operations as time_from, so using them is bit-identical to recomputing.
+struct DirConst {
+  float bearing[8];
+  float dist[8];
+};
+
+__device__ __forceinline__ void dir_consts(const JobDev &j, DirConst &d) {
+  const bool nu = j.north_up != 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int kk = k < 4 ? k : k + 1;
+    const int di = kk % 3 - 1, dj = kk / 3 - 1;
+    d.bearing[k] = bearing(di, dj, 0, 0, nu);
+    d.dist[k] = cell_distance(di, dj, j.gdx, j.gdy);
+  }
+}
+
+// Travel time of the direct spread from a cell with fire f to the cell it is
+// neighbour k of: the distance over the elliptical speed along that bearing,
+// the operations of step_time without the start time, so that
+// ftime + travel_time(...) is bit-identical to step_time(ftime, ...).
+__device__ __forceinline__ float travel_time(const DirConst &dc, int k, const Fire &f) {
+  return __fmul_rn(dc.dist[k], __frcp_rd(__fmul_rn(f.speed_max, spread_factor(dc.bearing[k], f))));
+}
+
 // ---------------------------------------------------------------- prep ----
 // Boundary bits (find_boundaries) packed with a warp ballot, plus the initial
-// state: time = FLT_MAX, no reference, empty referrer boxes.
+// state: time = FLT_MAX, no reference, empty referrer boxes; and the
+// direct-spread travel times toward the 8 neighbours (when the job has them).
 __global__ void __launch_bounds__(256) prep_kernel(const JobDev *__restrict__ jobs) {
   const JobDev j = jobs[blockIdx.y];
+  __shared__ DirConst dc;
+  if (threadIdx.x == 0) dir_consts(j, dc);
+  __syncthreads();
   const int64_t N = (int64_t)j.W * j.H;
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -86,6 +118,10 @@ __global__ void __launch_bounds__(256) prep_kernel(const JobDev *__restrict__ jo
           const Fire nb{__ldg(j.speed + n), __ldg(j.az + n), __ldg(j.ecc + n)};
           b |= !similar_fires(nb, me) && me.speed_max < nb.speed_max;
         }
+      }
+      if (j.tt && me.speed_max != 0.0f) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) j.tt[k * j.tt_plane + i] = travel_time(dc, k, me);
       }
       j.time[i] = FLT_MAX;
       j.refs[i] = kNoRef;
@@ -137,26 +173,6 @@ __device__ __noinline__ bool line_blocked_call(const uint32_t *__restrict__ bnd,
   return line_blocked(bnd, W, fx, fy, tx, ty, steps);
 }
 
-// Per-scenario constants of the eight neighbour directions, in the
-// reference's neighbour order (j outer, i inner, centre skipped): the bearing
-// from the neighbour to the cell and their distance, computed with the same
-// operations as time_from, so using them is bit-identical to recomputing.
-struct DirConst {
-  float bearing[8];
-  float dist[8];
-};
-
-__device__ __forceinline__ void dir_consts(const JobDev &j, DirConst &d) {
-  const bool nu = j.north_up != 0;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int kk = k < 4 ? k : k + 1;
-    const int di = kk % 3 - 1, dj = kk / 3 - 1;
-    d.bearing[k] = bearing(di, dj, 0, 0, nu);
-    d.dist[k] = cell_distance(di, dj, j.gdx, j.gdy);
-  }
-}
-
 struct Counters {
   uint32_t dda = 0, gat = 0, walk_max = 0;
   unsigned long long evals = 0, scans = 0, scan_cells = 0;
@@ -198,13 +214,15 @@ __device__ __forceinline__ Best evaluate_coop(const JobDev &j, const DirConst &d
   float nt = FLT_MAX, rt = FLT_MAX;
   uint32_t nr = kNoRef;
   Fire f{0.0f, 0.0f, 0.0f};
+  float tt = 0.0f;
   if (valid && nx >= 0 && ny >= 0 && nx < j.W && ny < j.H) {
-    // the three fire loads go out together with the state load (one memory
+    // the fire loads go out together with the state load (one memory
     // round trip), whether or not the neighbour turns out to burn
     const int64_t n = nx + (int64_t)ny * j.W;
     f.speed_max = __ldg(j.speed + n);
     f.azimuth_max = __ldg(j.az + n);
     f.eccentricity = __ldg(j.ecc + n);
+    if (j.tt) tt = __ldg(j.tt + k * j.tt_plane + n);
     acc.cell(nx, ny, nt, nr);
     act = nt < j.max_time && f.speed_max != 0.0f && !(ref_x(nr) == x && ref_y(nr) == y);
     if (act) rt = acc.time_of(nr);
@@ -214,8 +232,7 @@ __device__ __forceinline__ Best evaluate_coop(const JobDev &j, const DirConst &d
   uint32_t oref = 0, steps = 0;
   bool walked = false;
   if (act) {
-    const float ntime =
-        step_time(nt, dc.dist[k], __fmul_rn(f.speed_max, spread_factor(dc.bearing[k], f)));
+    const float ntime = j.tt ? __fadd_rn(nt, tt) : __fadd_rn(nt, travel_time(dc, k, f));
     cand = time_from(ref_x(nr), ref_y(nr), rt, x, y, f, j.gdx, j.gdy, j.north_up != 0);
     offer = ntime;
     oref = pack_ref(nx, ny);

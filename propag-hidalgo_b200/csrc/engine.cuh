@@ -25,6 +25,11 @@ struct JobDev {
   uint32_t pad;
   uint16_t *out_rx, *out_ry;
   uint32_t *out_bnd;   // caller's boundary output (may alias bnd)
+  // Direct-spread travel time of every cell toward each of its 8 neighbours
+  // (plane k: toward the cell whose neighbour k it is), written by the prep
+  // pass; null = computed per evaluation instead.  Plane stride tt_plane.
+  float *tt;
+  int64_t tt_plane;
 };
 
 struct Update {

@@ -219,9 +219,10 @@ extern "C" int64_t propag_server_submit(propag_server *s, const PropagJob *job,
     r.terrain = *terrain;
     r.has_terrain = true;
   }
-  // engine scratch (20 B per cell) + fire rasters + outputs, when the caller
-  // does not say
-  r.bytes = device_bytes ? device_bytes : (uint64_t)job->width * job->height * 64u;
+  // engine scratch (references and referrer boxes 20 B, travel times 32 B,
+  // boundary bits) + fire rasters 12 B + outputs 8 B per cell, when the
+  // caller does not say
+  r.bytes = device_bytes ? device_bytes : (uint64_t)job->width * job->height * 96u;
   r.res.submit_ns = now_ns();
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return PROPAG_ERR_INVALID;
