@@ -781,7 +781,14 @@ struct BoxExact {
 
 struct SmemGeom {
   int x0, y0, TW, TH, P, HR, C, rank, rows_mine;
-  int sh;  // box_shift: 0 when the halo side fits a byte, else 1
+  int sh;    // box_shift: 0 when the halo side fits a byte, else 1
+  int lc;    // log2 C (cluster sizes are powers of two): row hy -> CTA hy & (C-1), local row hy >> lc
+  uint32_t pm;  // ceil(2^32 / P): s / P = umulhi(s, pm), exact for s < 2^16 and P < 2^12
+  __device__ __forceinline__ int owner(int hy) const { return hy & (C - 1); }
+  __device__ __forceinline__ int lrow(int hy) const { return hy >> lc; }
+  uint32_t tm;  // the same for TW
+  __device__ __forceinline__ int div_p(int s) const { return (int)__umulhi((uint32_t)s, pm); }
+  __device__ __forceinline__ int div_tw(int s) const { return (int)__umulhi((uint32_t)s, tm); }
 };
 
 template <typename T>
@@ -796,8 +803,8 @@ __device__ __forceinline__ void mark3x3_smem(const SmemTile &sm, const SmemGeom 
   for (int t = 0; t < 9; ++t) {
     const int ax = hx + t % 3 - 1, ay = hy + t / 3 - 1;
     if (t == 4 || ax < 1 || ay < 1 || ax > g.TW || ay > g.TH) continue;
-    const int owner = ay % g.C;
-    const uint32_t li = (uint32_t)((ay / g.C) * g.P + ax);
+    const int owner = g.owner(ay);
+    const uint32_t li = (uint32_t)(g.lrow(ay) * g.P + ax);
     uint32_t *d = owner == g.rank ? sm.dirty : rank_ptr(sm.dirty, owner);
     atomicOr(d + (li >> 5), 1u << (li & 31));
   }
@@ -805,8 +812,8 @@ __device__ __forceinline__ void mark3x3_smem(const SmemTile &sm, const SmemGeom 
 
 __device__ __forceinline__ void smem_cell(const SmemTile &sm, const SmemGeom &g, int hx, int hy,
                                           float &t, uint32_t &r) {
-  const int owner = hy % g.C;
-  const int li = (hy / g.C) * g.P + hx;
+  const int owner = g.owner(hy);
+  const int li = g.lrow(hy) * g.P + hx;
   if (owner == g.rank) {
     t = sm.time[li];
     r = sm.ref[li];
@@ -820,8 +827,8 @@ __device__ __forceinline__ float smem_time_of(const JobDev &j, const SmemTile &s
                                               const SmemGeom &g, uint32_t r) {
   const int hx = ref_x(r) - (g.x0 - 1), hy = ref_y(r) - (g.y0 - 1);
   if (hx >= 0 && hy >= 0 && hx < g.P && hy < g.HR) {
-    const int owner = hy % g.C;
-    const int li = (hy / g.C) * g.P + hx;
+    const int owner = g.owner(hy);
+    const int li = g.lrow(hy) * g.P + hx;
     return owner == g.rank ? sm.time[li] : rank_ptr(sm.time, owner)[li];
   }
   return __ldcg(j.time + ref_x(r) + (int64_t)ref_y(r) * j.W);  // outside: static this launch
@@ -852,6 +859,9 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
   g.P = td.TW + 2;
   g.HR = td.TH + 2;
   g.C = (int)cluster.num_blocks();
+  g.lc = __ffs(g.C) - 1;
+  g.pm = (uint32_t)(0xFFFFFFFFu / (uint32_t)g.P) + 1u;
+  g.tm = (uint32_t)(0xFFFFFFFFu / (uint32_t)g.TW) + 1u;
   g.rank = (int)cluster.block_rank();
   g.rows_mine = g.HR > g.rank ? (g.HR - g.rank + g.C - 1) / g.C : 0;
   g.sh = (sizeof(BoxT) == 4 && (g.P > 256 || g.HR > 256)) ? 1 : 0;
@@ -864,7 +874,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
   // ---- stage the tile and its halo (state; referrer boxes restricted to
   // the staged region, where this launch's scans look) ----
   for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
-    const int lr = s / g.P, hx = s % g.P;
+    const int lr = g.div_p(s), hx = s - lr * g.P;
     const int hy = g.rank + lr * g.C;
     const int gx = g.x0 - 1 + hx, gy = g.y0 - 1 + hy;
     float t = FLT_MAX;
@@ -927,9 +937,9 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
       int x = 0, y = 0;
       Best own{FLT_MAX, kNoRef};
       if (valid) {
-        s = first ? (uint32_t)((lr_first + (int)ci / g.TW) * g.P + 1 + (int)ci % g.TW)
+        s = first ? (uint32_t)((lr_first + g.div_tw((int)ci)) * g.P + 1 + ((int)ci - g.div_tw((int)ci) * g.TW))
                   : list_get(sm, ci);
-        const int hx = (int)s % g.P, hy = g.rank + ((int)s / g.P) * g.C;
+        const int lr = g.div_p((int)s), hx = (int)s - lr * g.P, hy = g.rank + lr * g.C;
         x = g.x0 - 1 + hx;
         y = g.y0 - 1 + hy;
         own = Best{sm.time[s], sm.ref[s]};
@@ -965,7 +975,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
         uint32_t s, r;
         float t;
         upd_get(sm, u, s, t, r);
-        const int hx = (int)s % g.P, hy = g.rank + ((int)s / g.P) * g.C;
+        const int lr = g.div_p((int)s), hx = (int)s - lr * g.P, hy = g.rank + lr * g.C;
         const int x = g.x0 - 1 + hx, y = g.y0 - 1 + hy;
         sm.time[s] = t;
         sm.ref[s] = r;
@@ -974,8 +984,8 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
         // grid-wide box in global memory
         const int rhx = ref_x(r) - (g.x0 - 1), rhy = ref_y(r) - (g.y0 - 1);
         if (rhx >= 0 && rhy >= 0 && rhx < g.P && rhy < g.HR) {
-          const int owner = rhy % g.C;
-          const int li = (rhy / g.C) * g.P + rhx;
+          const int owner = g.owner(rhy);
+          const int li = g.lrow(rhy) * g.P + rhx;
           // the staged box is rounded outwards, so it may hold (x, y) already
           // while the grid-wide box does not: mark the slot for the merge
           // either way
@@ -1026,7 +1036,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
   // (rounded outwards: a box may cover a cell more than its referrers, which
   // costs scan work, never a missed referrer) ----
   for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
-    const int lr = s / g.P, hx = s % g.P;
+    const int lr = g.div_p(s), hx = s - lr * g.P;
     const int hy = g.rank + lr * g.C;
     const int gx = g.x0 - 1 + hx, gy = g.y0 - 1 + hy;
     if (gx < 0 || gy < 0 || gx >= j.W || gy >= j.H) continue;
