@@ -798,15 +798,28 @@ __device__ __forceinline__ T *rank_ptr(T *local, int r) {
 
 // Marks the tile cells of the 3x3 neighbourhood of halo cell (hx, hy) in
 // their owners' dirty bitmaps (fire-and-forget reductions on shared memory).
+// A row's (up to) three cells are consecutive slots of one owner: one
+// reduction, two where they straddle a word.
 __device__ __forceinline__ void mark3x3_smem(const SmemTile &sm, const SmemGeom &g, int hx, int hy) {
+  const int xa = max(hx - 1, 1), xb = min(hx + 1, g.TW);  // tile columns (halo coordinates)
+  if (xa > xb) return;
 #pragma unroll
-  for (int t = 0; t < 9; ++t) {
-    const int ax = hx + t % 3 - 1, ay = hy + t / 3 - 1;
-    if (t == 4 || ax < 1 || ay < 1 || ax > g.TW || ay > g.TH) continue;
+  for (int dy = -1; dy <= 1; ++dy) {
+    const int ay = hy + dy;
+    if (ay < 1 || ay > g.TH) continue;
+    uint32_t run = (1u << (xb - xa + 1)) - 1u;
+    if (dy == 0 && hx >= xa && hx <= xb) run &= ~(1u << (hx - xa));
+    if (!run) continue;
     const int owner = g.owner(ay);
-    const uint32_t li = (uint32_t)(g.lrow(ay) * g.P + ax);
+    const uint32_t l0 = (uint32_t)(g.lrow(ay) * g.P + xa);
     uint32_t *d = owner == g.rank ? sm.dirty : rank_ptr(sm.dirty, owner);
-    atomicOr(d + (li >> 5), 1u << (li & 31));
+    const uint32_t w = l0 >> 5, b = l0 & 31;
+    const uint32_t lo = run << b;
+    if (lo) atomicOr(d + w, lo);
+    if (b + (uint32_t)(xb - xa) >= 32) {
+      const uint32_t hi = run >> (32 - b);
+      if (hi) atomicOr(d + w + 1, hi);
+    }
   }
 }
 
