@@ -72,12 +72,17 @@ __device__ __forceinline__ DF two_sum(float a, float b) {
   return DF{s, e};
 }
 
-// sum_k (chi[k] + clo[k]) * m[k] as a double-float: exact products (fma) and
-// sums (two-sum), so that moisture sums keep ~2^-44 relative accuracy.
-__device__ __forceinline__ DF dot5_df(const float *chi, const float *clo, const float m[5]) {
+// sum_{k in [K0, K1)} (chi[k] + clo[k]) * m[k] as a double-float: exact
+// products (fma) and sums (two-sum), so that moisture sums keep ~2^-44
+// relative accuracy.  The catalog's dead-moisture and live-extinction
+// coefficients are zero for the live classes (3, 4) and the live-moisture
+// coefficients for the dead classes (0-2); zero terms leave hi and lo
+// unchanged, so summing only [K0, K1) gives the same bits.
+template <int K0, int K1>
+__device__ __forceinline__ DF dot_df(const float *chi, const float *clo, const float m[5]) {
   float hi = 0.0f, lo = 0.0f;
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
+  for (int k = K0; k < K1; ++k) {
     const float p = __fmul_rn(chi[k], m[k]);
     const float pe = __fmaf_rn(chi[k], m[k], -p);
     const DF s = two_sum(hi, p);
@@ -118,14 +123,14 @@ template <bool kFull>
 __device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], float ws,
                                           float waz, float slope, float aspect, FireOut &o) {
   // rx_int_rbqig
-  const DF dead = dot5_df(F.A, F.A_lo, m);
-  const DF live = dot5_df(F.B, F.B_lo, m);
+  const DF dead = dot_df<0, 3>(F.A, F.A_lo, m);
+  const DF live = dot_df<3, 5>(F.B, F.B_lo, m);
   const float rbqig = F.R0 + dot5(F.R, m);
   const DF mext{F.mext, F.mext_lo};
   const float eta_dead = eta_m(dead, mext);
   DF live_mext{0.0f, 0.0f};
   if (F.has_live != 0.0f) {
-    live_mext = df_sub(DF{F.LM0, F.LM0_lo}, dot5_df(F.LM, F.LM_lo, m));
+    live_mext = df_sub(DF{F.LM0, F.LM0_lo}, dot_df<0, 3>(F.LM, F.LM_lo, m));
     if (!(df_sub(live_mext, mext).hi > 0.0f)) live_mext = mext;  // max(live_mext, mext)
   }
   const float eta_live = eta_m(live, live_mext);
@@ -248,6 +253,15 @@ __global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, uint6
 cudaError_t upload_catalog() {
   FuelConst table[kMaxFuels];
   build_catalog_table(table);
+  // the kernel's moisture sums skip the classes whose coefficients are zero
+  for (int f = 0; f < kMaxFuels; ++f) {
+    for (int k = kHerb; k <= kWood; ++k)
+      if (table[f].A[k] != 0.0f || table[f].A_lo[k] != 0.0f || table[f].LM[k] != 0.0f ||
+          table[f].LM_lo[k] != 0.0f)
+        return cudaErrorInvalidValue;
+    for (int k = kD1; k <= kD100; ++k)
+      if (table[f].B[k] != 0.0f || table[f].B_lo[k] != 0.0f) return cudaErrorInvalidValue;
+  }
   return cudaMemcpyToSymbol(c_catalog, table, sizeof(table));
 }
 
