@@ -102,7 +102,7 @@ __device__ __forceinline__ DF df_sub(DF a, DF b) {
 __device__ __forceinline__ float eta_m(DF moist, DF mext) {
   const DF d = df_sub(mext, moist);
   if (!(d.hi > 0.0f)) return 0.0f;  // life_moist >= life_mext
-  const float u = __fdiv_rn(d.hi + d.lo, mext.hi + mext.lo);
+  const float u = __fdividef(d.hi + d.lo, mext.hi + mext.lo);  // 2 ulp; operands in [2^-126, 2^126]
   return u * fmaf(u, fmaf(u, 3.52f, -5.45f), 2.93f);
 }
 
@@ -135,7 +135,7 @@ __device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], 
   }
   const float eta_live = eta_m(live, live_mext);
   const float rx = fmaf(F.rx_alive, eta_live, F.rx_dead * eta_dead);
-  const float speed0 = __fdiv_rn(rx * F.flux_ratio, rbqig);
+  const float speed0 = __fdividef(rx * F.flux_ratio, rbqig);
 
   // calculate_wind_dependent_vars
   const float phi_slope = F.slope_k * slope * slope;
@@ -169,7 +169,7 @@ __device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], 
     sincosf(split, &sn, &cs);
     const float x = fmaf(phi_wind, cs, phi_slope);
     const float y = phi_wind * sn;
-    pew = hypotf(x, y);
+    pew = sqrtf(fmaf(x, x, y * y));  // phi values far below 1e18: no overflow to guard
     smax = speed0 * (1.0f + pew);
     ew = pow_pos(pew * F.wind_e, F.wind_b_inv);
     const float al = atan2f(fabsf(y), fabsf(x));
@@ -189,7 +189,7 @@ __device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], 
   const float a = 0.002840909f * ew;
   o.speed_max = smax * kFpmToMps;
   o.azimuth_max = az;
-  o.eccentricity = __fdiv_rn(sqrtf(a * (2.0f + a)), 1.0f + a);
+  o.eccentricity = __fdividef(sqrtf(a * (2.0f + a)), 1.0f + a);
   if (kFull) {  // the remaining FireCuda fields, Byram and flame
     o.rx_int = rx * kRxToSI;
     o.speed0 = speed0 * kFpmToMps;
