@@ -258,8 +258,9 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     tw[i] = std::min<int>(T, (int)j.width);
     th[i] = std::min<int>(T, (int)j.height);
     off[i] = job_bytes;
-    // references, referrer boxes, boundary bits, 8 travel-time planes
-    job_bytes += align_up(N * 4, 256) * 13 + (j.boundaries ? 0 : align_up(words * 4, 256));
+    // references, referrer boxes, boundary bits, 8 travel-time planes, the
+    // second state copy (time, references) of global-memory tiles
+    job_bytes += align_up(N * 4, 256) * 15 + (j.boundaries ? 0 : align_up(words * 4, 256));
     max_cells = std::max<uint64_t>(max_cells, N);
   }
   CK(e->job_scratch.reserve(job_bytes, stream));
@@ -280,6 +281,10 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     if (!jobs[i].boundaries) o += align_up(((N + 31) / 32) * 4, 256);
     jd[i].tt = e->job_scratch.at<float>(o);
     jd[i].tt_plane = (int64_t)(align_up(N * 4, 256) / 4);
+    o += 8 * align_up(N * 4, 256);
+    jd[i].time1 = e->job_scratch.at<float>(o);
+    o += align_up(N * 4, 256);
+    jd[i].refs1 = e->job_scratch.at<uint32_t>(o);
   }
   // ---- cluster size and tile residency ----
   // A tile launch runs in the cluster's shared memory when the tile and its
@@ -372,7 +377,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   const size_t upd_max = tn_max + 32 * (team_ctas + 1);
   const size_t ovf_list_bytes = align_up((size_t)csize * ovf_cap * 2, 256);
   const size_t ovf_upd_bytes = align_up((size_t)csize * ovf_cap * sizeof(Update), 256);
-  const size_t slot_bytes = align_up(words_max * 4, 256) + align_up(upd_max * sizeof(Update), 256) +
+  // two dirty bitmaps and two update arrays (by sweep parity)
+  const size_t slot_bytes = 2 * align_up(words_max * 4, 256) + 2 * align_up(upd_max * sizeof(Update), 256) +
                             256 + ovf_list_bytes + ovf_upd_bytes;
   CK(e->slot_scratch.reserve(slot_bytes * n_slots, stream));
   // meta: jobs, slots, stats, queue
@@ -409,9 +415,11 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     size_t o = slot_bytes * s;
     SlotDev &sd = e->slots_pinned[s];
     sd.dirty = e->slot_scratch.at<uint32_t>(o);
-    o += align_up(words_max * 4, 256);
+    sd.dirty_words = (uint32_t)(align_up(words_max * 4, 256) / 4);
+    sd.pad0 = 0;
+    o += 2 * align_up(words_max * 4, 256);
     sd.upd = e->slot_scratch.at<Update>(o);
-    o += align_up(upd_max * sizeof(Update), 256);
+    o += 2 * align_up(upd_max * sizeof(Update), 256);
     sd.ctr = e->slot_scratch.at<uint32_t>(o);
     o += 256;
     sd.ovf_list = e->slot_scratch.at<uint16_t>(o);
@@ -420,7 +428,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     sd.ovf_cap = (uint32_t)ovf_cap;
     sd.pad = 0;
     // the dirty bitmap and counters must start cleared
-    CK(cudaMemsetAsync(sd.dirty, 0, words_max * 4, stream));
+    CK(cudaMemsetAsync(sd.dirty, 0, 2 * align_up(words_max * 4, 256), stream));
     CK(cudaMemsetAsync(sd.ctr, 0, 64, stream));  // counters and barrier arrivals
   }
   JobDev *d_jobs = e->meta.at<JobDev>(0);

@@ -125,6 +125,10 @@ __global__ void __launch_bounds__(256) prep_kernel(const JobDev *__restrict__ jo
       }
       j.time[i] = FLT_MAX;
       j.refs[i] = kNoRef;
+      if (j.time1) {
+        j.time1[i] = FLT_MAX;
+        j.refs1[i] = kNoRef;
+      }
       j.box_x0[i] = kEmptyBox;
       j.box_y0[i] = kEmptyBox;
       j.box_x1[i] = 0u;
@@ -159,6 +163,10 @@ __global__ void ignite_kernel(const JobDev *__restrict__ jobs) {
       j.box_x0[c] = j.box_x1[c] = ign[k].x;
       j.box_y0[c] = j.box_y1[c] = ign[k].y;
     }
+    if (j.time1) {  // the second state copy starts equal
+      j.time1[c] = j.time[c];
+      j.refs1[c] = j.refs[c];
+    }
   }
 }
 
@@ -192,13 +200,15 @@ struct Counters {
 // the reference's order exactly.  Called by all 32 lanes.
 struct GlobalAcc {
   const JobDev &j;
+  const float *time;  // the state copy this sweep reads
+  const uint32_t *refs;
   __device__ __forceinline__ void cell(int x, int y, float &t, uint32_t &r) const {
     const int64_t n = x + (int64_t)y * j.W;
-    t = __ldcg(j.time + n);
-    r = __ldcg(j.refs + n);
+    t = __ldcg(time + n);
+    r = __ldcg(refs + n);
   }
   __device__ __forceinline__ float time_of(uint32_t r) const {
-    return __ldcg(j.time + ref_x(r) + (int64_t)ref_y(r) * j.W);
+    return __ldcg(time + ref_x(r) + (int64_t)ref_y(r) * j.W);
   }
 };
 
@@ -452,15 +462,28 @@ struct TileDesc {
 };
 
 // ================================================ global-memory tiles ====
-// The tile's state stays in global memory (L2).  The cells are dealt to the
-// team's R CTAs by 32-cell words of the tile's dirty bitmap, word w to CTA
-// w % R.  In the evaluate phase a CTA compacts the marked cells of its words
-// (all its cells on the first sweep) into a work list in shared memory, a
-// chunk of blockDim.x words at a time, evaluates them and appends its
-// improvements to its own region of the slot's update array; in the commit
-// phase it commits those improvements itself.  Marks for the next sweep set
-// bits in the bitmap with reductions (no return value), so the only global
-// atomic a sweep needs per CTA is the improvement count that ends the launch.
+// The tile's state stays in global memory (L2), in two copies X0 (the job's
+// arrays) and X1: sweep s reads X[s & 1] and writes X[(s + 1) & 1], so that a
+// sweep is a single phase between two team barriers.  The cells are dealt to
+// the team's R CTAs by 32-cell words of the dirty bitmap, word w to CTA
+// w % R, and only a cell's owner writes it.  In sweep s a CTA
+//   1. compacts the marked cells of its words in bitmap D[s & 1] (all its
+//      cells on the first sweep) into a work list in shared memory, a chunk
+//      of blockDim.x words at a time, clearing the words;
+//   2. evaluates them against X[s & 1] and appends its improvements to its
+//      update region of parity s & 1;
+//   3. copies its improvements of sweep s - 1 (already in X[s & 1]) into
+//      X[(s + 1) & 1], then writes this sweep's improvements there, marks
+//      the 3x3 neighbourhoods of the burning ones in D[(s + 1) & 1] and scans
+//      their referrer boxes (reading X[s & 1]);
+//   4. adds its improvement count to the team's and meets the team.
+// After a sweep without improvements both copies hold the same state.  Marks
+// are bit reductions without a return value; the improvement count is the
+// only global atomic a CTA makes per sweep.  The referrer scans read the
+// references as the sweep started: a referrer whose reference changes in this
+// sweep improved, so its neighbourhood is marked anyway, and one that did not
+// reads the same reference either way -- the marks are those of scans run
+// after the commits.
 
 // Marks the 3x3 neighbourhood of tile cell (lx, ly), centre excluded, in the
 // dirty bitmap: per row the (up to) three cells are consecutive bits, so a
@@ -515,12 +538,27 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
   const uint32_t TN = (uint32_t)TW * (uint32_t)TH;
   const uint32_t nwords = (TN + 31) / 32;
   const uint32_t mine = nwords > rank ? (nwords - rank + R - 1) / R : 0u;  // words of this CTA
-  Update *const upd = s.upd + (size_t)rank * global_tile_upd_cap(TN, R);
+  const uint32_t cap = global_tile_upd_cap(TN, R);
+  float *const tm[2] = {j.time, j.time1};
+  uint32_t *const rf[2] = {j.refs, j.refs1};
   bool first = true, worked = false;
-  int p = 0;
+  uint32_t prev_upd = 0;  // this CTA's improvements of the previous sweep
+  int p = 0;              // sweep parity: read X[p], write X[p ^ 1]
+  // The team's improvement count of a sweep rotates over three counters
+  // (s.ctr[5..7]): the one of sweep s - 1 is cleared after sweep s's barrier,
+  // when every CTA has read it and none can add to it before the next barrier.
+  int q = 0;
   for (;;) {
     ++cx.sweeps;  // every thread counts, so the abort below is uniform
-    // ---- evaluate (Jacobi: nothing is written to the state) ----
+    const float *const rt = tm[p];
+    const uint32_t *const rr = rf[p];
+    float *const wt = tm[p ^ 1];
+    uint32_t *const wr = rf[p ^ 1];
+    uint32_t *const dirty = s.dirty + (size_t)p * s.dirty_words;
+    uint32_t *const dirty_next = s.dirty + (size_t)(p ^ 1) * s.dirty_words;
+    Update *const upd = s.upd + ((size_t)p * R + rank) * cap;
+    const Update *const upd_prev = s.upd + ((size_t)(p ^ 1) * R + rank) * cap;
+    // ---- 1, 2: compact and evaluate (nothing is written to X[p]) ----
     if (threadIdx.x == 0) cta_ctr[1] = 0;
     for (uint32_t c0 = 0; c0 < mine; c0 += blockDim.x) {
       __syncthreads();  // the previous chunk's list is consumed
@@ -533,8 +571,8 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
         if (first) {
           bits = (w == nwords - 1 && (TN & 31)) ? (1u << (TN & 31)) - 1u : 0xFFFFFFFFu;
         } else {
-          bits = __ldcg(s.dirty + w);
-          if (bits) s.dirty[w] = 0u;
+          bits = __ldcg(dirty + w);
+          if (bits) dirty[w] = 0u;
         }
       }
       uint32_t at = warp_append(cta_ctr + 0, __popc(bits), lane);
@@ -555,9 +593,9 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
           x = x0 + (int)(k % (uint32_t)TW);
           y = y0 + (int)(k / (uint32_t)TW);
           const int64_t c = x + (int64_t)y * j.W;
-          own = Best{__ldcg(j.time + c), __ldcg(j.refs + c)};
+          own = Best{__ldcg(rt + c), __ldcg(rr + c)};
         }
-        const Best b = evaluate_coop(j, dc, GlobalAcc{j}, x, y, own, valid, lane, cx.cnt);
+        const Best b = evaluate_coop(j, dc, GlobalAcc{j, rt, rr}, x, y, own, valid, lane, cx.cnt);
         const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
         const uint32_t ai = warp_append(cta_ctr + 1, improved ? 1u : 0u, lane);
         if (improved) upd[ai] = Update{k, b.time, b.ref, 0u};
@@ -565,26 +603,17 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
     }
     __syncthreads();
     const uint32_t my_upd = cta_ctr[1];
-    if (threadIdx.x == 0 && my_upd) atomicAdd(s.ctr + 2 + p, my_upd);
-    if (!team.sync()) {
-      cx.failed = cx.abort = true;
-      break;
+    // ---- 3a: the previous sweep's improvements into X[p ^ 1] ----
+    for (uint32_t u = threadIdx.x; u < prev_upd; u += blockDim.x) {
+      const uint4 raw = __ldcg(reinterpret_cast<const uint4 *>(upd_prev) + u);  // Update{k, time, ref}
+      const int64_t c = (x0 + (int)(raw.x % (uint32_t)TW)) + (int64_t)(y0 + (int)(raw.x / (uint32_t)TW)) * j.W;
+      wt[c] = __uint_as_float(raw.y);
+      wr[c] = raw.z;
     }
-    cx.tick(first ? 0 : 1);
-    const uint32_t nupd = __ldcg(s.ctr + 2 + p);
-    // the other parity's count, last read before the previous commit
-    // barrier, is cleared for the next sweep (also when this launch ends, so
-    // that the next tile launch finds both at zero)
-    if (cx.leader) s.ctr[2 + (p ^ 1)] = 0;
-    if (nupd == 0) break;
-    worked = true;
-    // ---- commit (update_point / commit_point), mark, referrer scans ----
-    // A referrer scan may run while other cells of this sweep commit: a cell
-    // whose reference changes in this sweep is itself marked, and a box only
-    // grows, so what the scan must find (referrers from earlier sweeps) is
-    // unaffected by the concurrent writes.  Updates are dealt `per` to a
-    // warp, as few as spreads them over the CTA's warps (a warp's referrer
-    // scans run one after another).
+    __syncthreads();  // this sweep's improvements of the same cells land after
+    // ---- 3b: commit (update_point / commit_point), mark, referrer scans.
+    // Updates are dealt `per` to a warp, as few as spreads them over the
+    // CTA's warps (a warp's referrer scans run one after another).
     const uint32_t per = min(32u, (my_upd + nwarps - 1) / nwarps);
     for (uint32_t base = warp * per; base < my_upd; base += nwarps * per) {
       const uint32_t u = base + lane;
@@ -599,11 +628,11 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
         ly = (int)(raw.x / (uint32_t)TW);
         const int x = x0 + lx, y = y0 + ly;
         const int64_t c = x + (int64_t)y * j.W;
-        j.time[c] = ut;
-        j.refs[c] = raw.z;
+        wt[c] = ut;
+        wr[c] = raw.z;
         box_expand_global(j, raw.z, x, y);
         // only a burning cell is read by its neighbours
-        if (ut < j.max_time && __ldg(j.speed + c) != 0.0f) mark3x3_bits(s.dirty, lx, ly, TW, TH);
+        if (ut < j.max_time && __ldg(j.speed + c) != 0.0f) mark3x3_bits(dirty_next, lx, ly, TW, TH);
         want = pack_ref(x, y);
         const uint32_t bx0 = __ldcg(j.box_x0 + c);
         if (bx0 != kEmptyBox)
@@ -614,20 +643,30 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
           scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cx.cnt,
           [&](int xx, int yy, float &t) {
             const int64_t n = xx + (int64_t)yy * j.W;
-            t = __ldcg(j.time + n);
-            return __ldcg(j.refs + n);
+            t = __ldcg(rt + n);
+            return __ldcg(rr + n);
           },
           [&](bool hit, int xx, int yy) {
-            if (hit) mark3x3_bits(s.dirty, xx - x0, yy - y0, TW, TH);
+            if (hit) mark3x3_bits(dirty_next, xx - x0, yy - y0, TW, TH);
           });
     }
+    // ---- 4: count, meet ----
+    if (threadIdx.x == 0 && my_upd) atomicAdd(s.ctr + 5 + q, my_upd);
     if (!team.sync()) {
       cx.failed = cx.abort = true;
       break;
     }
-    cx.tick(2);
+    cx.tick(first ? 0 : 1);
+    const uint32_t nupd = __ldcg(s.ctr + 5 + q);
+    // the previous sweep's count (zero when this launch ends here, so that
+    // the next tile launch finds all three at zero)
+    if (cx.leader) s.ctr[5 + (q == 0 ? 2 : q - 1)] = 0;
+    if (nupd == 0) break;  // X[p ^ 1] got the last improvements: both copies agree
+    worked = true;
     if (cx.leader) cx.improvements += nupd;
+    prev_upd = my_upd;
     p ^= 1;
+    q = q == 2 ? 0 : q + 1;
     first = false;
     if (cx.sweeps > cx.max_sweeps) {
       cx.abort = true;
@@ -1109,6 +1148,7 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
       taken = atomicAdd(queue, 1u);
       s.ctr[4] = taken;
       s.ctr[0] = s.ctr[1] = s.ctr[2] = s.ctr[3] = 0;
+      s.ctr[5] = s.ctr[6] = s.ctr[7] = 0;
     }
     if (!team.sync()) break;
     // teams take the jobs in queue order; `order` (when given) maps queue

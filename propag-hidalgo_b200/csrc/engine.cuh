@@ -30,6 +30,10 @@ struct JobDev {
   // pass; null = computed per evaluation instead.  Plane stride tt_plane.
   float *tt;
   int64_t tt_plane;
+  // Second copy of the state for global-memory tiles (sweeps alternate
+  // between the copies); null when every tile is resident in shared memory.
+  float *time1;
+  uint32_t *refs1;
 };
 
 struct Update {
@@ -41,16 +45,19 @@ struct Update {
 static_assert(sizeof(Update) == 16, "an update is read back as one 16-byte load");
 
 // Global-memory scratch of one team slot.  dirty/upd serve tile launches
-// whose state stays in global memory: the tile's dirty bitmap and the
-// update array, CTA r of the team using entries from r * cap on (cap =
-// global_tile_upd_cap); ovf_list/ovf_upd take the work-list and update-list
+// whose state stays in global memory: the tile's dirty bitmaps and the
+// update arrays (one per sweep parity), CTA r of an R-CTA team using entries
+// from (parity * R + r) * cap on (cap = global_tile_upd_cap); ovf_list/ovf_upd take the work-list and update-list
 // entries of shared-memory tiles beyond their shared-memory capacity
 // (ovf_cap entries per CTA of the cluster, CTA r at offset r * ovf_cap).
 struct SlotDev {
-  uint32_t *dirty;
+  uint32_t *dirty;        // two bitmaps of dirty_words words (by sweep parity)
+  uint32_t dirty_words;
+  uint32_t pad0;
   Update *upd;
-  // [0..1] unused, [2..3] update counts (by sweep parity), [4] job,
-  // [8..9] group-mode barrier arrivals (64-bit)
+  // [0..3] shared-memory tiles' counters, [4] job, [5..7] global-memory
+  // tiles' improvement counts (rotating by sweep), [8..9] group-mode barrier
+  // arrivals (64-bit)
   uint32_t *ctr;
   uint16_t *ovf_list;
   Update *ovf_upd;
