@@ -161,7 +161,8 @@ typedef struct PropagOptions {
   int32_t tile;    /* default super-grid tile side; 0 = PROPAG_DEFAULT_TILE,
                       PROPAG_TILE_WHOLE_GRID = one tile for the whole grid */
   int32_t cluster; /* CTAs (one cluster) cooperating on one scenario, 1..16; 0 = auto;
-                      PROPAG_CLUSTER_GROUPS = group mode (below) */
+                      PROPAG_CLUSTER_GROUPS = group mode (below); -N (N > 1):
+                      group mode with teams of at least N CTAs */
   int32_t threads; /* threads per CTA, multiple of 32, <= 512; 0 = 512 */
   int32_t device;  /* CUDA device ordinal; -1 = the current device */
 } PropagOptions;

@@ -169,8 +169,8 @@ extern "C" propag_engine *propag_engine_create(const PropagOptions *opt) {
   cudaGetDevice(&e->device);
   e->sms = sms;
   if (opt) {
-    if ((opt->cluster < 0 && opt->cluster != PROPAG_CLUSTER_GROUPS) || opt->cluster > 16) {
-      fail(PROPAG_ERR_INVALID, "cluster must be 0..16 or PROPAG_CLUSTER_GROUPS");
+    if (opt->cluster < -1024 || opt->cluster > 16) {
+      fail(PROPAG_ERR_INVALID, "cluster must be 0..16, PROPAG_CLUSTER_GROUPS or -(team size)");
       delete e;
       return nullptr;
     }
@@ -292,17 +292,17 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   const size_t budget = e->smem_budget;
   auto fits = [&](uint32_t i, int c) { return smem_bytes(tw[i], th[i], c) <= budget; };
   int csize = e->csize;
-  if (csize == 0) {
-    // A few scenarios run fastest in group mode: one runs on one cluster at
-    // most (its tiles go one after another), so a cluster leaves most SMs idle,
-    // while teams of 37-148 CTAs spread each sweep over the whole device.
-    // Measured on B200 (1024^2 ensemble members): 1 scenario 79 ms in group
-    // mode against 120 ms on a 16-CTA cluster, 8 scenarios 162 against
-    // 194 ms; from 16 scenarios on, clusters are faster.
+  if (csize == 0 && e->auto_groups) {
+    // Group mode, one team per job of max(4, CTAs / jobs) CTAs.  A scenario
+    // runs on one cluster at most in cluster mode (its tiles go one after
+    // another), so few scenarios leave most SMs idle, while a group-mode team
+    // spreads each sweep over its CTAs with one barrier per sweep.  Measured
+    // on B200, 1024^2 ensemble members: 1 member 79 ms in group mode against
+    // 120 ms on a 16-CTA cluster; 64 members 408 ms (teams of 8) against
+    // 514 (8-CTA clusters); 256 members 1 082 ms (teams of 4) against 1 531.
     int ctas = 0;
     CK(engine_max_clusters(1, e->threads, global_tile_smem(e->threads), &ctas));
-    if (e->auto_groups && ctas >= 64 && n_jobs <= (uint32_t)(2 * std::max(1, ctas / 32)))
-      csize = PROPAG_CLUSTER_GROUPS;
+    if (ctas >= 8) csize = -std::max(4, ctas / (int)std::max<uint32_t>(n_jobs, 1));
   }
   if (csize == 0) {
     // among the cluster sizes that hold every job's tile, the one that runs
@@ -336,14 +336,16 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   }
   size_t smem = 0, tn_max = 1, ovf_cap = 0;
   uint32_t n_slots = 0, group = 0;
-  if (csize == PROPAG_CLUSTER_GROUPS) {
+  if (csize <= PROPAG_CLUSTER_GROUPS) {
     // group mode: the co-resident CTAs split into teams of at least 32 CTAs
-    // (one team per job up to that), tiles in global memory
+    // (or of -csize CTAs when given), one team per job up to that, tiles in
+    // global memory
     smem = global_tile_smem(e->threads);
     int ctas = 0;
     CK(engine_max_clusters(1, e->threads, smem, &ctas));
     if (ctas < 2) return fail(PROPAG_ERR_CUDA, "group mode needs at least 2 resident CTAs");
-    n_slots = std::min<uint32_t>(n_jobs, (uint32_t)std::max(1, ctas / 32));
+    const int team = csize == PROPAG_CLUSTER_GROUPS ? 32 : std::max(2, -csize);
+    n_slots = std::min<uint32_t>(n_jobs, (uint32_t)std::max(1, ctas / team));
     group = (uint32_t)ctas / n_slots;
     for (uint32_t i = 0; i < n_jobs; ++i) {
       jd[i].smem_tile = kSmemTileGlobal;
@@ -696,7 +698,10 @@ extern "C" int propag_autotune(const PropagJob *jobs, const PropagTerrainPtrs *t
     if (all) cands.push_back(c);
   }
   if (cands.empty()) cands.push_back(16);  // global-memory tiles: the largest cluster
-  cands.push_back(PROPAG_CLUSTER_GROUPS);
+  // group mode: the automatic team size and teams of 16, 8 and 4 CTAs
+  cands.push_back(0);
+  for (int t : {16, 8, 4})
+    if ((uint32_t)t * n_jobs > (uint32_t)sms) cands.push_back(-t);  // else the automatic one
   cudaEvent_t a = nullptr, b = nullptr;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));

@@ -21,6 +21,7 @@ PROPAG_ERR_OOM = -5
 PROPAG_DEFAULT_TILE = 323
 PROPAG_TILE_WHOLE_GRID = -1
 PROPAG_CLUSTER_GROUPS = -1  # PropagOptions.cluster: teams of CTAs over the whole device
+SERVER_DEFAULT_BYTES_PER_CELL = 96  # a request's device memory when submit gets 0
 
 
 class GT(C.Structure):

@@ -47,11 +47,12 @@ def _uneven(n=6, seed=41):
     return S.config3(n=n, seed=seed, min_size=48, max_size=360)
 
 
-@pytest.mark.parametrize("cluster", [0, 16, -1])
+@pytest.mark.parametrize("cluster", [0, 16, -1, -4])
 def test_graph_replays_equal_single_runs(pp, cluster):
     """Six uneven scenarios captured once and replayed twice, with the
-    automatic choice (group mode for this few), 16-CTA clusters and group
-    mode (a cooperative launch inside the graph)."""
+    automatic choice (group mode), 16-CTA clusters, group mode with the
+    automatic team size and with teams of 4 CTAs (a cooperative launch inside
+    the graph)."""
     import torch
     from py_propag import _lib as L
     scs = _uneven()
@@ -103,7 +104,9 @@ def test_autotune_picks_a_fitting_cluster_and_results_do_not_change(pp):
     tiles = [0] * len(scs)
     jobs, terrains, keep = _device_batch(pp, L, scs, tiles)
     opts, ms = pp.autotune(jobs, terrains, repeats=1)
-    assert opts["cluster"] in (1, 2, 4, 8, 16, -1) and ms > 0
+    # cluster sizes whose shared memory holds the tiles, the automatic choice
+    # (0: group mode) and group-mode teams of 16, 8 or 4 CTAs
+    assert opts["cluster"] in (1, 2, 4, 8, 16, 0, -16, -8, -4) and ms > 0
     g = pp.Graph(jobs, terrains, cluster=opts["cluster"])
     g.launch()
     torch.cuda.synchronize()

@@ -180,10 +180,11 @@ def _device_scenario(pp, sc):
     return dev
 
 
-@pytest.mark.parametrize("cluster", [1, 4, 16, -1])
+@pytest.mark.parametrize("cluster", [1, 4, 16, -1, -2])
 def test_batch_equals_single_runs(pp, oracle, cluster):
     """Uneven scenarios in one persistent launch give each scenario's own
-    result, whatever the cluster size (-1: group mode, four teams)."""
+    result, whatever the cluster size (-1: group mode, four teams; -2: teams
+    of 2+ CTAs)."""
     import torch
     from py_propag import _lib as L
     from py_propag import scenarios as S

@@ -60,7 +60,7 @@ def test_budget_and_bad_requests(pp):
     from py_propag import _lib as L
     scs = _uneven(n=2, seed=53)
     jobs, terrains, keep = _device_batch(pp, L, scs, [0, 0])
-    small = min(sc.width * sc.height for sc in scs) * 64
+    small = min(sc.width * sc.height for sc in scs) * L.SERVER_DEFAULT_BYTES_PER_CELL
     srv = pp.Server(hbm_budget=small, lanes=2)
     big = int(np.argmax([sc.width * sc.height for sc in scs]))
     rid = srv.submit(jobs[big], terrains[big])
