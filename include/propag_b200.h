@@ -141,12 +141,13 @@ typedef struct PropagIgnition {
 } PropagIgnition;
 
 /* PropagOptions.cluster: group mode.  The engine's co-resident CTAs split
- * into teams of at least 32 (one per scenario, up to that), launched
- * cooperatively without clusters; a team keeps its tiles in global memory and
- * meets at a counter barrier in global memory whose waits are bounded (a wait
- * that gives up fails the run with PROPAG_ERR_TIMEOUT).  One scenario then
- * runs on the whole device instead of one cluster.  Results are identical in
- * every mode. */
+ * into teams of at least 32 (PROPAG_CLUSTER_GROUPS) or N (cluster = -N) CTAs,
+ * one per scenario up to that, launched cooperatively without clusters; a
+ * team keeps its tiles in global memory and meets at a counter barrier in
+ * global memory whose waits are bounded (a wait that gives up fails the run
+ * with PROPAG_ERR_TIMEOUT).  One scenario then runs on the whole device
+ * instead of one cluster.  cluster = 0 chooses group mode with teams of
+ * max(4, CTAs / scenarios).  Results are identical in every mode. */
 #define PROPAG_CLUSTER_GROUPS (-1)
 
 /* Self-test of group mode's bounded wait (no reference counterpart): runs an
