@@ -10,11 +10,12 @@
 //   Terrain::upslope                                 firelib.rs:400-409
 //   Byram's intensity, flame length                  firelib.rs:424-441
 //
-// Layout and mapping: every thread handles 4 consecutive cells with 128-bit
-// loads of each of the nine float rasters and one 32-bit load of the fuel
-// codes, and 128-bit stores of each output; the grid is a multiple of the SM
-// count and strides over the rasters.  The fuel table sits in shared memory
-// (14 models x 40 floats), indexed per cell.
+// Layout and mapping: one cell per thread, grid-stride, so that every load
+// and store of a warp is one coalesced run (4 bytes per lane, 1 for the fuel
+// codes); the grid is a multiple of the SM count.  The fuel table sits in
+// shared memory (20 models x 64 floats), indexed per cell.  Double-float
+// moisture sums measured faster here than FP64 ones (0.33-0.35 ms against
+// 0.35-0.36 ms at 4096^2).
 //
 // FP32 formulation.  The arithmetic is the reference's, rearranged where the
 // float evaluation of the literal formula loses accuracy against double:
