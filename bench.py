@@ -55,6 +55,12 @@ FIRE_BYTES_PER_CELL = 49  # 37 B in (u8 fuel + 9 f32) + 12 B out (3 f32)
 # the GPU leg reports whether its own count still agrees.
 WORK_EVALUATIONS = {"config1": 264061772}
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# one single-pass ncu capture of the full-size workload; the command and the
+# figures are in profiles/dram_traffic_config1-4096.md.
+DRAM_TRAFFIC = {"config1": {"engine_kernel": 5.58e9 + 0.36089e9,
+                            "fire_kernel": 557.95e6 + 181.74e6}}
+
 
 def _peaks():
     try:
@@ -605,10 +611,12 @@ def bench_b200(args):
         "cells_per_s": N * world * args.steps / (total_ms / 1e3),
         "e2e": e2e,
         "roofline": {"bound": "hbm", "kernel": "engine_kernel (propagation)", "achieved": ach,
-                     "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": None,
+                     "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                     "traffic": DRAM_TRAFFIC.get(args.workload, {}).get("engine_kernel"),
                      "algorithmic_bytes": prop_bytes, "peak_source": peak_kind},
         "kernels": {"fire_kernel": {"achieved": fire_ach, "peak": peak, "unit": "GB/s",
-                                    "frac": fire_ach / peak, "bytes": FIRE_BYTES_PER_CELL * N}},
+                                    "frac": fire_ach / peak, "bytes": FIRE_BYTES_PER_CELL * N,
+                                    "traffic": DRAM_TRAFFIC.get(args.workload, {}).get("fire_kernel")}},
         "workload_stats": stats,
         "work_matches_recorded": (stats["evaluations"] == known) if known else None,
         "gpu_launches": 5 * args.steps,
