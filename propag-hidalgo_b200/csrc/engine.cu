@@ -176,7 +176,7 @@ struct Best {
   uint32_t ref;
 };
 
-__device__ __noinline__ bool line_blocked_call(const uint32_t *__restrict__ bnd, int W, int fx,
+__device__ __forceinline__ bool line_blocked_call(const uint32_t *__restrict__ bnd, int W, int fx,
                                                int fy, int tx, int ty, uint32_t &steps) {
   return line_blocked(bnd, W, fx, fy, tx, ty, steps);
 }
@@ -541,6 +541,8 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
   const uint32_t cap = global_tile_upd_cap(TN, R);
   float *const tm[2] = {j.time, j.time1};
   uint32_t *const rf[2] = {j.refs, j.refs1};
+  // the launch's counters in registers (the context may live in local memory)
+  Counters cnt = cx.cnt;
   bool first = true, worked = false;
   uint32_t prev_upd = 0;  // this CTA's improvements of the previous sweep
   int p = 0;              // sweep parity: read X[p], write X[p ^ 1]
@@ -579,7 +581,7 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
       for (; bits; bits &= bits - 1) list[at++] = (uint16_t)(threadIdx.x * 32 + __ffs(bits) - 1);
       __syncthreads();
       const uint32_t nlist = cta_ctr[0];
-      if (threadIdx.x == 0) cx.cnt.evals += nlist;
+      if (threadIdx.x == 0) cnt.evals += nlist;
       // four cells per warp, eight lanes per cell
       for (uint32_t base = warp * 4; base < nlist; base += nwarps * 4) {
         const uint32_t ci = base + (lane >> 3);
@@ -595,7 +597,7 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
           const int64_t c = x + (int64_t)y * j.W;
           own = Best{__ldcg(rt + c), __ldcg(rr + c)};
         }
-        const Best b = evaluate_coop(j, dc, GlobalAcc{j, rt, rr}, x, y, own, valid, lane, cx.cnt);
+        const Best b = evaluate_coop(j, dc, GlobalAcc{j, rt, rr}, x, y, own, valid, lane, cnt);
         const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
         const uint32_t ai = warp_append(cta_ctr + 1, improved ? 1u : 0u, lane);
         if (improved) upd[ai] = Update{k, b.time, b.ref, 0u};
@@ -640,7 +642,7 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
                          (int)__ldcg(j.box_y1 + c), x0, y0, TW, TH, j.W, j.H);
       }
       warp_scan_boxes(
-          scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cx.cnt,
+          scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cnt,
           [&](int xx, int yy, float &t) {
             const int64_t n = xx + (int64_t)yy * j.W;
             t = __ldcg(rt + n);
@@ -673,6 +675,7 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
       break;
     }
   }
+  cx.cnt = cnt;
   return worked;
 }
 
@@ -957,6 +960,8 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
   team.sync(false);
   cx.tick(3);
 
+  // the launch's counters in registers (the context may live in local memory)
+  Counters cnt = cx.cnt;
   bool first = true, worked = false;
   int par = 0;
   for (;;) {
@@ -980,7 +985,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
     }
     __syncthreads();
     const uint32_t nlist = first ? (uint32_t)(in_rows * g.TW) : sm.ctr[0];
-    if (threadIdx.x == 0) cx.cnt.evals += nlist;
+    if (threadIdx.x == 0) cnt.evals += nlist;
     // four cells per warp, eight lanes per cell
     for (uint32_t base = (threadIdx.x >> 5) * 4; base < nlist; base += (blockDim.x >> 5) * 4) {
       const uint32_t ci = base + (lane >> 3);
@@ -996,7 +1001,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
         y = g.y0 - 1 + hy;
         own = Best{sm.time[s], sm.ref[s]};
       }
-      const Best b = evaluate_coop(j, dc, SmemAcc{j, sm, g}, x, y, own, valid, lane, cx.cnt);
+      const Best b = evaluate_coop(j, dc, SmemAcc{j, sm, g}, x, y, own, valid, lane, cnt);
       const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
       const uint32_t at = warp_append(sm.ctr + 1, improved ? 1u : 0u, lane);
       if (improved) upd_put(sm, at, s, b.time, b.ref);
@@ -1062,7 +1067,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
         }
       }
       warp_scan_boxes(
-          scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cx.cnt,
+          scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cnt,
           [&](int xx, int yy, float &t) {
             uint32_t r;
             smem_cell(sm, g, xx - (g.x0 - 1), yy - (g.y0 - 1), t, r);
@@ -1109,6 +1114,7 @@ __device__ bool tile_smem(const JobDev &j, const DirConst &dc, char *smem, const
   if (threadIdx.x == 0) sm.ctr[0] = sm.ctr[1] = 0u;
   team.sync();
   cx.tick(3);
+  cx.cnt = cnt;
   return worked;
 }
 
