@@ -1,6 +1,6 @@
 // Arrival-time propagation on B200: boundary/prep pass, ignition scatter,
-// the persistent cluster engine and the post mask.
-//
+// the persistent engine and the post mask.
+
 // Reference semantics (paths relative to the reference project):
 //   pre_propagate / find_boundaries   crates/propag/src/propag.cu:345-375,410-421
 //   propag / Propagator::run          crates/propag/src/propag.cu:62-109,382-394
@@ -22,20 +22,23 @@
 //     scanning that box only.
 // The first sweep of each tile launch evaluates the whole tile.
 //
-// Mapping.  One thread-block cluster works on one scenario at a time and
-// pulls scenarios from a queue, so a batch of scenarios runs concurrently,
-// each on its own cluster, in one launch.  A sweep is two phases separated by
-// cluster barriers: evaluate (reads only) and commit (writes the state, marks
-// the next sweep's cells, scans referrer boxes).  Cluster barriers are
-// hardware barriers: there is no spin-wait anywhere.
-//
-// A tile launch runs in one of two modes:
-//   * shared-memory tile: the tile and its halo (time, reference, referrer
-//     boxes) are staged into the distributed shared memory of the cluster,
-//     rows dealt round-robin to the CTAs; all sweeps read and write there and
-//     the tile is written back at the end of the launch;
-//   * global tile (tiles too large for the cluster's shared memory): the state
-//     stays in global memory and the work lists in the slot's scratch.
+// Mapping.  The engine is one persistent launch whose CTAs form teams; a
+// team works on one scenario at a time and pulls scenarios from a queue
+// (largest first), so a batch runs concurrently, scenario per team.  Two
+// kinds of team:
+//   * cluster mode: a thread-block cluster of 1-16 CTAs.  The tile and its
+//     halo (time, reference, referrer boxes) are staged into the cluster's
+//     distributed shared memory, rows dealt round-robin to the CTAs; a sweep
+//     is two phases, evaluate (reads only) and commit (writes the state,
+//     marks the next sweep's cells, scans referrer boxes), separated by
+//     hardware cluster barriers, and the tile is written back at the end of
+//     the launch.  Tiles too large for the cluster's shared memory take the
+//     global-memory path below.
+//   * group mode: a cooperative launch without clusters whose CTAs form
+//     teams of any size (the whole device for one scenario).  The tile state
+//     stays in global memory in two copies, so that a sweep is one phase; the
+//     team meets at a counter barrier in global memory whose wait is bounded
+//     (the engine's only spin-wait; see Team).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
