@@ -12,7 +12,8 @@
 //
 // Layout and mapping: one cell per thread, grid-stride, so that every load
 // and store of a warp is one coalesced run (4 bytes per lane, 1 for the fuel
-// codes); the grid is a multiple of the SM count.  The fuel table sits in
+// codes); the grid holds as many CTAs as are resident at once (one wave),
+// and 32-bit indices serve every grid below 2^32 cells.  The fuel table sits in
 // shared memory (20 models x 64 floats), indexed per cell.  Double-float
 // moisture sums measured faster here than FP64 ones (0.33-0.35 ms against
 // 0.35-0.36 ms at 4096^2).
@@ -212,17 +213,20 @@ struct Outputs {
   float *f[10];  // PropagFireFields order
 };
 
-__device__ __forceinline__ void store_cell(const Outputs &out, uint64_t i, const FireOut &o) {
+// kFull: every field whose output is given; else the three the propagation
+// needs (the 3-field entry point passes only those).
+template <bool kFull, typename Index>
+__device__ __forceinline__ void store_cell(const Outputs &out, Index i, const FireOut &o) {
   const float v[10] = {o.rx_int, o.speed0, o.hpua, o.phi_eff_wind, o.speed_max,
                        o.azimuth_max, o.eccentricity, o.residence_time, o.byrams, o.flame};
 #pragma unroll
   for (int k = 0; k < 10; ++k)
-    if (out.f[k]) out.f[k][i] = v[k];
+    if ((kFull || (k >= 4 && k <= 6)) && out.f[k]) out.f[k][i] = v[k];
 }
 
-template <bool kFull>
+template <bool kFull, typename Index>
 __device__ __forceinline__ void one_cell(const FuelConst *cat, const Inputs &in, const Outputs &out,
-                                         uint64_t i) {
+                                         Index i) {
   const uint8_t code = __ldg(in.fuel + i);
   FireOut o{};
   if (code < kMaxFuels && cat[code].has_fire != 0.0f) {
@@ -231,7 +235,7 @@ __device__ __forceinline__ void one_cell(const FuelConst *cat, const Inputs &in,
     burn_cell<kFull>(cat[code], m, __ldg(in.ws + i), __ldg(in.waz + i), __ldg(in.slope + i),
                      __ldg(in.aspect + i), o);
   }
-  store_cell(out, i, o);
+  store_cell<kFull>(out, i, o);
 }
 
 // One cell per thread, grid-stride: every load and store is coalesced (4 or
@@ -239,15 +243,41 @@ __device__ __forceinline__ void one_cell(const FuelConst *cat, const Inputs &in,
 // kernel small in the instruction cache.  kFull: all ten fields; else the
 // three the propagation needs (the shared fields are the same operations,
 // so both give bit-identical values for them).
-template <bool kFull>
-__global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, uint64_t n) {
+// Index: uint32_t when n + the grid's threads fit in 32 bits (cheaper
+// address arithmetic), else uint64_t.
+template <bool kFull, typename Index>
+__global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, Index n) {
   __shared__ FuelConst cat[kMaxFuels];
   for (int t = threadIdx.x; t < (int)(sizeof(cat) / 4); t += blockDim.x)
     reinterpret_cast<float *>(cat)[t] = reinterpret_cast<const float *>(c_catalog)[t];
   __syncthreads();
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+  const Index stride = (Index)gridDim.x * blockDim.x;
+  for (Index i = (Index)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     one_cell<kFull>(cat, in, out, i);
+}
+
+// CTAs of fire_kernel<kFull, Index> resident per SM (registers limit it).
+template <bool kFull, typename Index>
+static int fire_ctas_per_sm(int threads) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fire_kernel<kFull, Index>, threads, 0) !=
+          cudaSuccess ||
+      n < 1)
+    n = 1;
+  return n;
+}
+
+template <bool kFull, typename Index>
+static cudaError_t launch_fire_t(const Inputs &in, const Outputs &out, uint64_t n, int sm_count,
+                                 int threads, cudaStream_t stream) {
+  // one wave: as many CTAs as are resident at once, each striding over an
+  // equal share (a second, partial wave would leave SMs idle at the end)
+  uint64_t blocks = (n + threads - 1) / threads;
+  const uint64_t cap = (uint64_t)sm_count * (uint64_t)fire_ctas_per_sm<kFull, Index>(threads);
+  if (blocks > cap) blocks = cap;
+  if (blocks == 0) blocks = 1;
+  fire_kernel<kFull, Index><<<(unsigned)blocks, threads, 0, stream>>>(in, out, (Index)n);
+  return cudaGetLastError();
 }
 
 // ---- host-side launchers (called from api.cpp) ------------------------------
@@ -275,13 +305,13 @@ cudaError_t launch_fire(bool full, uint64_t n, const uint8_t *fuel, const float 
   for (int k = 0; k < 10; ++k) out.f[k] = outs[k];
   if (n == 0) return cudaSuccess;
   const int threads = 256;
-  uint64_t blocks = (n + threads - 1) / threads;
-  const uint64_t cap = (uint64_t)sm_count * 8;  // 8 resident blocks per SM
-  if (blocks > cap) blocks = cap;
-  if (blocks == 0) blocks = 1;
-  if (full) fire_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
-  else fire_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(in, out, n);
-  return cudaGetLastError();
+  // 32-bit indices while the last index plus one grid stride stays below 2^32
+  const bool narrow = n + (uint64_t)sm_count * 8 * threads < (1ull << 32);
+  if (full)
+    return narrow ? launch_fire_t<true, uint32_t>(in, out, n, sm_count, threads, stream)
+                  : launch_fire_t<true, uint64_t>(in, out, n, sm_count, threads, stream);
+  return narrow ? launch_fire_t<false, uint32_t>(in, out, n, sm_count, threads, stream)
+                : launch_fire_t<false, uint64_t>(in, out, n, sm_count, threads, stream);
 }
 
 }  // namespace propag
