@@ -698,9 +698,11 @@ extern "C" int propag_autotune(const PropagJob *jobs, const PropagTerrainPtrs *t
     if (all) cands.push_back(c);
   }
   if (cands.empty()) cands.push_back(16);  // global-memory tiles: the largest cluster
-  // group mode: the automatic team size and teams of 16, 8 and 4 CTAs
+  // group mode: the automatic team size and teams of 24, 16, 8 and 4 CTAs
+  // (64 uneven scenarios on B200: 350 ms with teams of 24, 373 with 16,
+  // 493 with 32)
   cands.push_back(0);
-  for (int t : {16, 8, 4})
+  for (int t : {24, 16, 8, 4})
     if ((uint32_t)t * n_jobs > (uint32_t)sms) cands.push_back(-t);  // else the automatic one
   cudaEvent_t a = nullptr, b = nullptr;
   CK(cudaEventCreate(&a));

@@ -105,8 +105,8 @@ def test_autotune_picks_a_fitting_cluster_and_results_do_not_change(pp):
     jobs, terrains, keep = _device_batch(pp, L, scs, tiles)
     opts, ms = pp.autotune(jobs, terrains, repeats=1)
     # cluster sizes whose shared memory holds the tiles, the automatic choice
-    # (0: group mode) and group-mode teams of 16, 8 or 4 CTAs
-    assert opts["cluster"] in (1, 2, 4, 8, 16, 0, -16, -8, -4) and ms > 0
+    # (0: group mode) and group-mode teams of 24, 16, 8 or 4 CTAs
+    assert opts["cluster"] in (1, 2, 4, 8, 16, 0, -24, -16, -8, -4) and ms > 0
     g = pp.Graph(jobs, terrains, cluster=opts["cluster"])
     g.launch()
     torch.cuda.synchronize()
