@@ -499,6 +499,9 @@ extern "C" int propag_engine_run(propag_engine *e, const PropagJob *jobs, uint32
 extern "C" int propag_selftest_group_wait(uint32_t *status) {
   if (!status) return fail(PROPAG_ERR_INVALID, "null status");
   *status = 0;
+  int sms = 0;
+  const int rc0 = ensure_device(-1, &sms);  // no device: PROPAG_ERR_NO_DEVICE
+  if (rc0) return rc0;
   PropagOptions o{0, PROPAG_CLUSTER_GROUPS, 0, -1};
   propag_engine *e = propag_engine_create(&o);
   if (!e) return PROPAG_ERR_CUDA;  // message set by propag_engine_create

@@ -73,6 +73,34 @@ def test_struct_layouts(L):
     assert C.sizeof(L.PropagIgnition) == 12
 
 
+def _header_defines():
+    out = {}
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        for m in re.finditer(r"^#define\s+(PROPAG_[A-Z_0-9]+)\s+\(?(-?\d+)[uU]?\)?", open(h).read(), re.M):
+            out[m.group(1)] = int(m.group(2))
+    return out
+
+
+def test_extension_structs_and_constants_match_the_header(L):
+    # PropagStats (include/propag_b200.h): 13 u64 counters, status and
+    # max_walk u32, then 4 u64 (start/done clocks, scan cells, barrier wait)
+    assert C.sizeof(L.PropagStats) == 13 * 8 + 2 * 4 + 4 * 8
+    names = [f[0] for f in L.PropagStats._fields_]
+    assert names[-6:] == ["status", "max_walk", "t_start_ns", "t_done_ns", "scan_cells", "cyc_wait"]
+    d = _header_defines()
+    assert d["PROPAG_CLUSTER_GROUPS"] == L.PROPAG_CLUSTER_GROUPS == -1
+    assert d["PROPAG_DEFAULT_TILE"] == L.PROPAG_DEFAULT_TILE
+    assert d["PROPAG_ERR_TIMEOUT"] == L.PROPAG_ERR_TIMEOUT
+
+
+def test_group_wait_selftest_needs_a_device(lib, L, pp):
+    if pp.check_cuda_available():
+        pytest.skip("a GPU is present")
+    st = C.c_uint32(7)
+    assert lib.propag_selftest_group_wait(C.byref(st)) == L.PROPAG_ERR_NO_DEVICE
+    assert lib.propag_selftest_group_wait(None) != L.PROPAG_OK
+
+
 def _georef(pp, w=100, h=80, gt=(1000.0, 5.0, 0.0, 2000.0, 0.0, 5.0)):
     return pp.PyGeoReference(w, h, PROJ, list(gt))
 
