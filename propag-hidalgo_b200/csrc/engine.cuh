@@ -111,7 +111,7 @@ constexpr int kSmemFixedBytes = 256;
 constexpr int kSmemMaxSide = 510;  // halo side whose corners fit a byte at box_shift 1
 
 // JobDev::smem_tile
-constexpr int32_t kSmemTileGlobal = 0;  // state in global memory, work lists in the slot
+constexpr int32_t kSmemTileGlobal = 0;  // state in global memory (two copies), bitmaps and update regions in the slot
 constexpr int32_t kSmemTileCoarse = 1;  // shared memory, BoxCoarse referrer boxes
 constexpr int32_t kSmemTileExact = 2;   // shared memory, BoxExact referrer boxes
 
