@@ -50,10 +50,11 @@ FIRE_BYTES_PER_CELL = 49  # 37 B in (u8 fuel + 9 f32) + 12 B out (3 f32)
 # reference-time gather (algorithmic, neighbours reused on chip)
 
 # Propagation work of the full workloads (cell evaluations), as counted on the
-# device by the engine and identically by the CPU restatement (same schedule,
-# bit-identical results).  The CPU legs time a bounded crop and scale by it;
-# the GPU leg reports whether its own count still agrees.
-WORK_EVALUATIONS = {"config1": 264061772}
+# device by the engine in group mode (first sweeps over the pending cells
+# only) and identically by the CPU restatement in the same mode (full=2; same
+# schedule, bit-identical results).  The CPU legs time a bounded crop in that
+# mode and scale by it; the GPU leg reports whether its own count still agrees.
+WORK_EVALUATIONS = {"config1": 163564125}
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # one single-pass ncu capture of the full-size workload; the command and the
@@ -185,7 +186,7 @@ def cpu_baseline(sc, evaluations_full: int, threads: int, budget_s: float = 20.0
         tp = time.perf_counter()
         r = O.propagate(crop, crop, sc.dx, sc.dy, sc.max_time, f[:, 4].astype(np.float32),
                         f[:, 5].astype(np.float32), f[:, 6].astype(np.float32), ign,
-                        tile=323, threads=threads)
+                        tile=323, threads=threads, full=2)
         dt = time.perf_counter() - tp
         prop_rate = r.stats["evaluations"] / dt
         if time.perf_counter() - t0 > budget_s / 3 or crop >= 1024:

@@ -152,9 +152,12 @@ def initial_state(width: int, height: int, ignitions):
 
 def propagate(width: int, height: int, dx: float, dy: float, max_time: float,
               speed, az, ecc, ignitions=None, *, time0=None, refs0=None, tile: int = 0,
-              full: bool = False, trig: int = 0, threads: int = 0) -> OracleResult:
+              full: int = 0, trig: int = 0, threads: int = 0) -> OracleResult:
     """Runs the CPU restatement.  tile = cells per side of one cooperative
-    launch (block * grid_w); 0 = one tile (global Jacobi)."""
+    launch (block * grid_w); 0 = one tile (global Jacobi).  full: 0 = the
+    engine's work skipping (whole tile in a launch's first sweep), 1 = every
+    cell in every sweep, 2 = skipping in first sweeps too (grid-wide pending
+    bitmap); all three give the same results."""
     lib = _load()
     s_arr, a_arr, e_arr = (np.ascontiguousarray(x, dtype=np.float32).ravel() for x in (speed, az, ecc))
     if time0 is None:

@@ -33,6 +33,14 @@
  * propag.cu:221-224; every cell keeps the bounding box of the cells that ever
  * adopted it as their reference, and that box is scanned).  `full` = 1
  * evaluates the whole tile in every sweep; the tests check both modes agree.
+ * `full` = 2 also skips work in the first sweep of a launch: a grid-wide
+ * pending bitmap keeps the marks that fall outside the launching tile
+ * (neighbours of changed cells, and neighbours of referrers found by scanning
+ * the whole referrer box instead of the tile grown by one cell), starting
+ * from the neighbours of the burning cells; a launch's first sweep evaluates
+ * only the tile's pending cells.  A cell whose inputs did not change since
+ * its last evaluation cannot improve, so the results, improvements and sweep
+ * counts are those of the other modes (the evaluation counts are smaller).
  *
  * Intrinsics: __frcp_rd and __fsqrt_rz are emulated exactly (round-down
  * reciprocal, round-toward-zero square root).  The cosine and arctangent are
@@ -350,11 +358,35 @@ static inline void mark(uint8_t *dirty, int32_t *cand, int64_t *ncand, int TW, i
     }
 }
 
+/* Marks the eight neighbours of grid cell (gx, gy): inside the tile in the
+ * sweep's dirty list, outside it in the grid-wide pending bitmap (full = 2). */
+static inline void mark_grid(uint8_t *dirty, int32_t *cand, int64_t *ncand, uint8_t *pending,
+                             int W, int H, int x0, int y0, int TW, int TH, int gx, int gy) {
+  for (int j = -1; j < 2; j++)
+    for (int i = -1; i < 2; i++) {
+      if (i == 0 && j == 0) continue;
+      const int ax = gx + i, ay = gy + j;
+      if (ax < 0 || ay < 0 || ax >= W || ay >= H) continue;
+      const int lx = ax - x0, ly = ay - y0;
+      if (lx >= 0 && ly >= 0 && lx < TW && ly < TH) {
+        const int32_t kk = lx + ly * TW;
+        if (!dirty[kk]) {
+          dirty[kk] = 1;
+          cand[(*ncand)++] = kk;
+        }
+      } else {
+        pending[(int64_t)ax + (int64_t)ay * W] = 1;
+      }
+    }
+}
+
 /* One cooperative launch over the tile [x0,x1) x [y0,y1): Jacobi sweeps until
  * a sweep improves nothing (Propagator::run, propag.cu:62-109).  Returns 1 if
- * any sweep improved a cell (the launch's `worked` flag). */
+ * any sweep improved a cell (the launch's `worked` flag).  `pending` is the
+ * grid-wide bitmap of full = 2 (else NULL). */
 static int run_tile(world_t *w, box_t *refbox, int x0, int y0, int x1, int y1, int full,
-                    int64_t *stats, uint8_t *dirty, int32_t *cand, upd_t *upd, int32_t *chg) {
+                    int64_t *stats, uint8_t *dirty, int32_t *cand, upd_t *upd, int32_t *chg,
+                    uint8_t *pending) {
   const int W = (int)w->s->width, H = (int)w->s->height;
   const int TW = x1 - x0, TH = y1 - y0;
   const int64_t TN = (int64_t)TW * TH;
@@ -363,8 +395,40 @@ static int run_tile(world_t *w, box_t *refbox, int x0, int y0, int x1, int y1, i
   int64_t nchg = 0;
   for (;;) {
     int64_t ncand = 0;
-    if (full || first) {
+    if (first && pending) {
+      /* the tile's pending cells (their inputs changed since they were last
+       * evaluated) */
+      for (int64_t k = 0; k < TN; k++) {
+        const int64_t g = (int64_t)(x0 + k % TW) + (int64_t)(y0 + k / TW) * W;
+        if (pending[g]) {
+          pending[g] = 0;
+          cand[ncand++] = (int32_t)k;
+        }
+      }
+    } else if (full == 1 || first) {
       for (int64_t k = 0; k < TN; k++) cand[ncand++] = (int32_t)k;
+    } else if (pending) {
+      /* as below, with marks outside the tile kept in the pending bitmap and
+       * the whole referrer box scanned */
+      for (int64_t c = 0; c < nchg; c++) {
+        int32_t k = chg[c];
+        const int gx = x0 + k % TW, gy = y0 + k / TW;
+        const int64_t gc = (int64_t)gx + (int64_t)gy * W;
+        if (w->time[gc] < w->s->max_time && w->speed[gc] != 0.0f)
+          mark_grid(dirty, cand, &ncand, pending, W, H, x0, y0, TW, TH, gx, gy);
+        const box_t b = refbox[gc];
+        if (b.x0 > b.x1) continue;
+        stats[7]++;
+        for (int yy = b.y0; yy <= b.y1; yy++)
+          for (int xx = b.x0; xx <= b.x1; xx++) {
+            const int64_t n = (int64_t)xx + (int64_t)yy * W;
+            stats[8]++;
+            if (w->time[n] < w->s->max_time && w->speed[n] != 0.0f && w->rx[n] == (uint16_t)gx &&
+                w->ry[n] == (uint16_t)gy)
+              mark_grid(dirty, cand, &ncand, pending, W, H, x0, y0, TW, TH, xx, yy);
+          }
+      }
+      for (int64_t c = 0; c < ncand; c++) dirty[cand[c]] = 0;
     } else {
       /* cells whose inputs changed: the neighbours of every changed cell that
        * burns (a cell that does not burn is skipped by its neighbours), and
@@ -460,7 +524,8 @@ static int run_tile(world_t *w, box_t *refbox, int x0, int y0, int x1, int y1, i
  * 0xFFFF otherwise) and receive the result before the post mask.
  * tile = cells per side of one cooperative launch; tile <= 0 means one tile
  * for the whole grid.  full = 1 evaluates every cell of the tile in every
- * sweep (no work skipping).  Returns 0 on success. */
+ * sweep (no work skipping); full = 2 skips work in first sweeps too (see the
+ * top of this file).  Returns 0 on success. */
 int ops_propagate(const ops_settings_t *s, const float *speed, const float *az, const float *ecc,
                   float *time, uint16_t *rx, uint16_t *ry, const uint32_t *bnd, int tile, int full,
                   int trig, int threads, int64_t *stats) {
@@ -485,7 +550,18 @@ int ops_propagate(const ops_settings_t *s, const float *speed, const float *az, 
   int32_t *cand = (int32_t *)malloc(sizeof(int32_t) * (size_t)TN);
   int32_t *chg = (int32_t *)malloc(sizeof(int32_t) * (size_t)TN);
   upd_t *upd = (upd_t *)malloc(sizeof(upd_t) * (size_t)TN);
-  if (!refbox || !dirty || !cand || !chg || !upd) return -2;
+  uint8_t *pending = full == 2 ? (uint8_t *)calloc((size_t)N, 1) : NULL;
+  if (!refbox || !dirty || !cand || !chg || !upd || (full == 2 && !pending)) return -2;
+  if (pending) /* the neighbours of the burning cells can improve first */
+    for (int64_t i = 0; i < N; i++) {
+      if (!(time[i] < s->max_time && speed[i] != 0.0f)) continue;
+      const int x = (int)(i % W), y = (int)(i / W);
+      for (int j = -1; j < 2; j++)
+        for (int ii = -1; ii < 2; ii++) {
+          const int ax = x + ii, ay = y + j;
+          if ((ii || j) && ax >= 0 && ay >= 0 && ax < W && ay < H) pending[ax + (int64_t)ay * W] = 1;
+        }
+    }
   for (int64_t i = 0; i < N; i++) refbox[i] = (box_t){1, 1, 0, 0};
   for (int64_t i = 0; i < N; i++)
     if (time[i] < FLT_MAX) {
@@ -502,10 +578,11 @@ int ops_propagate(const ops_settings_t *s, const float *speed, const float *az, 
         int x0 = gx * T, y0 = gy * T;
         int x1 = x0 + T < W ? x0 + T : W, y1 = y0 + T < H ? y0 + T : H;
         stats[1]++;
-        any |= run_tile(&w, refbox, x0, y0, x1, y1, full, stats, dirty, cand, upd, chg);
+        any |= run_tile(&w, refbox, x0, y0, x1, y1, full, stats, dirty, cand, upd, chg, pending);
       }
     }
   } while (any);
+  free(pending);
   free(refbox);
   free(dirty);
   free(cand);

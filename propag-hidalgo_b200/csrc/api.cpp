@@ -259,8 +259,10 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     th[i] = std::min<int>(T, (int)j.height);
     off[i] = job_bytes;
     // references, referrer boxes, boundary bits, 8 travel-time planes, the
-    // second state copy (time, references) of global-memory tiles
-    job_bytes += align_up(N * 4, 256) * 15 + (j.boundaries ? 0 : align_up(words * 4, 256));
+    // second state copy (time, references) and the pending bitmap of
+    // global-memory tiles
+    job_bytes += align_up(N * 4, 256) * 15 + (j.boundaries ? 0 : align_up(words * 4, 256)) +
+                 align_up(words * 4, 256);
     max_cells = std::max<uint64_t>(max_cells, N);
   }
   CK(e->job_scratch.reserve(job_bytes, stream));
@@ -285,6 +287,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     jd[i].time1 = e->job_scratch.at<float>(o);
     o += align_up(N * 4, 256);
     jd[i].refs1 = e->job_scratch.at<uint32_t>(o);
+    o += align_up(N * 4, 256);
+    jd[i].pending = e->job_scratch.at<uint32_t>(o);  // kept below for global-memory tiles only
   }
   // ---- cluster size and tile residency ----
   // A tile launch runs in the cluster's shared memory when the tile and its
@@ -370,6 +374,12 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     if (max_clusters < 1) return fail(PROPAG_ERR_CUDA, "cluster size " + std::to_string(csize) + " cannot be resident");
     n_slots = std::min<uint32_t>(n_jobs, (uint32_t)max_clusters);
   }
+  // First sweeps skip unchanged cells (pending bitmap) on global-memory tiles
+  // of grids below 2^27 cells (a warp sums 32 referrer-box areas in 32 bits);
+  // shared-memory tiles evaluate the whole tile in a launch's first sweep.
+  for (uint32_t i = 0; i < n_jobs; ++i)
+    if (jd[i].smem_tile != kSmemTileGlobal || (uint64_t)jd[i].W * jd[i].H >= (1ull << 27))
+      jd[i].pending = nullptr;
   e->last_cluster = group ? PROPAG_CLUSTER_GROUPS : csize;
   e->last_group = group;
   e->last_smem = smem;

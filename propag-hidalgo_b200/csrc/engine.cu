@@ -138,7 +138,10 @@ __global__ void __launch_bounds__(256) prep_kernel(const JobDev *__restrict__ jo
       j.box_y1[i] = 0u;
     }
     const unsigned word = __ballot_sync(kFull, b);
-    if (lane == 0) j.bnd[w0 >> 5] = word;
+    if (lane == 0) {
+      j.bnd[w0 >> 5] = word;
+      if (j.pending) j.pending[w0 >> 5] = 0u;
+    }
   }
 }
 
@@ -169,6 +172,22 @@ __global__ void ignite_kernel(const JobDev *__restrict__ jobs) {
     if (j.time1) {  // the second state copy starts equal
       j.time1[c] = j.time[c];
       j.refs1[c] = j.refs[c];
+    }
+  }
+  // the neighbours of the burning cells are the cells that can improve first
+  if (j.pending) {
+    for (uint32_t k = 0; k < j.n_ignitions; ++k) {
+      if (ign[k].x >= (uint32_t)j.W || ign[k].y >= (uint32_t)j.H) continue;
+      const int64_t c = ign[k].x + (int64_t)ign[k].y * j.W;
+      if (!(j.time[c] < j.max_time && j.speed[c] != 0.0f)) continue;
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int ax = (int)ign[k].x + dx, ay = (int)ign[k].y + dy;
+          if ((dx || dy) && ax >= 0 && ay >= 0 && ax < j.W && ay < j.H) {
+            const int64_t n = ax + (int64_t)ay * j.W;
+            j.pending[n >> 5] |= 1u << (n & 31);
+          }
+        }
     }
   }
 }
@@ -512,6 +531,55 @@ __device__ __forceinline__ void mark3x3_bits(uint32_t *dirty, int lx, int ly, in
   }
 }
 
+// As mark3x3_bits, and the neighbours outside the tile (inside the grid) into
+// the grid-wide pending bitmap (one reduction per cell: only cells on or
+// beyond the tile's border have such neighbours).  (lx, ly) may lie anywhere
+// in the grid, relative to the tile's corner (x0, y0).
+__device__ __forceinline__ void mark3x3_pending(uint32_t *dirty, uint32_t *pending, const JobDev &j,
+                                                int x0, int y0, int lx, int ly, int TW, int TH) {
+  mark3x3_bits(dirty, lx, ly, TW, TH);
+  if (lx > 0 && ly > 0 && lx < TW - 1 && ly < TH - 1) return;
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    const int ax = lx + t % 3 - 1, ay = ly + t / 3 - 1;
+    if (t == 4 || (ax >= 0 && ay >= 0 && ax < TW && ay < TH)) continue;
+    const int gx = x0 + ax, gy = y0 + ay;
+    if (gx < 0 || gy < 0 || gx >= j.W || gy >= j.H) continue;
+    const int64_t g = gx + (int64_t)gy * j.W;
+    atomicOr(pending + (g >> 5), 1u << (g & 31));
+  }
+}
+
+// Takes (reads and clears) the pending bits of tile cells k0 .. k0 + n - 1
+// (n <= 32, tile-linear order) from the grid-wide bitmap; bit i of the
+// result is cell k0 + i.  The cells of one tile row are consecutive grid
+// cells, so each row segment is a funnel shift of two words.
+__device__ __forceinline__ uint32_t take_pending(uint32_t *pending, const JobDev &j, int x0, int y0,
+                                                 int TW, uint32_t k0, uint32_t n) {
+  uint32_t out = 0, done = 0;
+  while (done < n) {
+    const uint32_t k = k0 + done;
+    const uint32_t lx = k % (uint32_t)TW, ly = k / (uint32_t)TW;
+    const uint32_t seg = min(n - done, (uint32_t)TW - lx);  // cells left in this row
+    const int64_t g = (x0 + (int64_t)lx) + (int64_t)(y0 + (int64_t)ly) * j.W;
+    const int64_t wi = g >> 5;
+    const uint32_t sh = (uint32_t)(g & 31);
+    const bool two = sh + seg > 32;  // the segment reaches the next word (same row)
+    const uint64_t w2 =
+        (uint64_t)__ldcg(pending + wi) | (two ? (uint64_t)__ldcg(pending + wi + 1) << 32 : 0ull);
+    const uint32_t m = seg >= 32 ? 0xFFFFFFFFu : (1u << seg) - 1u;
+    const uint32_t bits = (uint32_t)(w2 >> sh) & m;
+    if (bits) {
+      const uint64_t cm = (uint64_t)bits << sh;
+      if ((uint32_t)cm) atomicAnd(pending + wi, ~(uint32_t)cm);
+      if ((uint32_t)(cm >> 32)) atomicAnd(pending + wi + 1, ~(uint32_t)(cm >> 32));
+    }
+    out |= bits << done;
+    done += seg;
+  }
+  return out;
+}
+
 struct SweepCtx {
   bool leader;
   Counters cnt;
@@ -574,7 +642,11 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
       if (t < mine) {
         const uint32_t w = rank + t * R;
         if (first) {
-          bits = (w == nwords - 1 && (TN & 31)) ? (1u << (TN & 31)) - 1u : 0xFFFFFFFFu;
+          const uint32_t nb = (w == nwords - 1 && (TN & 31)) ? (TN & 31) : 32u;
+          // the whole tile, or with a pending bitmap the cells whose inputs
+          // changed since their last evaluation
+          bits = j.pending ? take_pending(j.pending, j, x0, y0, TW, w * 32, nb)
+                           : (nb == 32 ? 0xFFFFFFFFu : (1u << nb) - 1u);
         } else {
           bits = __ldcg(dirty + w);
           if (bits) dirty[w] = 0u;
@@ -637,12 +709,27 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
         wr[c] = raw.z;
         box_expand_global(j, raw.z, x, y);
         // only a burning cell is read by its neighbours
-        if (ut < j.max_time && __ldg(j.speed + c) != 0.0f) mark3x3_bits(dirty_next, lx, ly, TW, TH);
+        if (ut < j.max_time && __ldg(j.speed + c) != 0.0f) {
+          if (j.pending)
+            mark3x3_pending(dirty_next, j.pending, j, x0, y0, lx, ly, TW, TH);
+          else
+            mark3x3_bits(dirty_next, lx, ly, TW, TH);
+        }
         want = pack_ref(x, y);
         const uint32_t bx0 = __ldcg(j.box_x0 + c);
-        if (bx0 != kEmptyBox)
-          box = clip_box((int)bx0, (int)__ldcg(j.box_y0 + c), (int)__ldcg(j.box_x1 + c),
-                         (int)__ldcg(j.box_y1 + c), x0, y0, TW, TH, j.W, j.H);
+        if (bx0 != kEmptyBox) {
+          if (j.pending)  // the whole box: referrers anywhere mark pending cells
+            // clamped to the grid: a box that another lane creates in this
+            // sweep can show the empty marker (0xFFFFFFFF, -1 as int) in its
+            // other corner; such a box had no referrers before this sweep,
+            // and this sweep's referrers mark their neighbourhoods themselves
+            box = Box{max((int)bx0, 0), max((int)__ldcg(j.box_y0 + c), 0),
+                      min((int)__ldcg(j.box_x1 + c), j.W - 1),
+                      min((int)__ldcg(j.box_y1 + c), j.H - 1)};
+          else
+            box = clip_box((int)bx0, (int)__ldcg(j.box_y0 + c), (int)__ldcg(j.box_x1 + c),
+                           (int)__ldcg(j.box_y1 + c), x0, y0, TW, TH, j.W, j.H);
+        }
       }
       warp_scan_boxes(
           scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cnt,
@@ -652,7 +739,11 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
             return __ldcg(rr + n);
           },
           [&](bool hit, int xx, int yy) {
-            if (hit) mark3x3_bits(dirty_next, xx - x0, yy - y0, TW, TH);
+            if (!hit) return;
+            if (j.pending)
+              mark3x3_pending(dirty_next, j.pending, j, x0, y0, xx - x0, yy - y0, TW, TH);
+            else
+              mark3x3_bits(dirty_next, xx - x0, yy - y0, TW, TH);
           });
     }
     // ---- 4: count, meet ----

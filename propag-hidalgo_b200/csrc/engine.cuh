@@ -34,6 +34,11 @@ struct JobDev {
   // between the copies); null when every tile is resident in shared memory.
   float *time1;
   uint32_t *refs1;
+  // Grid-wide pending bitmap of global-memory tiles (bit x + y W): cells whose
+  // inputs changed since they were last evaluated, outside the tile that
+  // changed them; a tile launch's first sweep evaluates only its pending
+  // cells.  Null: first sweeps evaluate the whole tile.
+  uint32_t *pending;
 };
 
 struct Update {

@@ -70,7 +70,9 @@ def test_graph_replays_equal_single_runs(pp, cluster):
             assert np.array_equal(b["time"].cpu().numpy().view(np.uint32),
                                   a.arrival_times.ravel().view(np.uint32)), (rep, i)
             assert np.array_equal(b["rx"].cpu().numpy().view(np.uint16), a.refs_x), (rep, i)
-            for k in ("sweeps", "evaluations", "improvements", "burned"):
+            # (evaluations are not compared: group-mode runs evaluate only
+            # the pending cells in first sweeps, shared-memory clusters all)
+            for k in ("sweeps", "improvements", "burned"):
                 assert st[i][k] == a.stats[k], (rep, i, k)
     g.close()
 

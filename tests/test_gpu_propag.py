@@ -17,6 +17,27 @@ pytestmark = pytest.mark.gpu
 FMAX = np.finfo(np.float32).max
 
 
+SCHEDULE = ("rounds", "launches", "sweeps", "improvements")
+WORK = ("evaluations", "dda_steps", "gathers")
+
+
+def _check_counts(res, o, rerun, keys=SCHEDULE + WORK):
+    """Schedule counters equal the oracle's; the work counters equal the
+    oracle's in the mode the engine used: whole first sweeps (shared-memory
+    tiles, oracle full=0) or first sweeps over the pending cells only
+    (global-memory tiles, oracle full=2; `rerun(full)` runs the oracle)."""
+    for k in keys:
+        if k not in WORK:
+            assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+    work = [k for k in keys if k in WORK]
+    if all(res.stats[k] == o.stats[k] for k in work):
+        return 0
+    o2 = rerun(2)
+    for k in work:
+        assert res.stats[k] == o2.stats[k], (k, res.stats[k], o.stats[k], o2.stats[k])
+    return 2
+
+
 def _fire(pp, terrain):
     f = pp.fire_behaviour(terrain, full=False)
     return f["speed_max"], f["azimuth_max"], f["eccentricity"]
@@ -32,8 +53,10 @@ def _check(pp, oracle, terrain, w, h, dx, dy, max_time, ignitions, tile):
     s = _settings(pp, w, h, dx, dy, max_time)
     res = pp.propagate_arrays(s, terrain, ignitions, tile=tile)
     sp, az, ec = _fire(pp, terrain)
-    o = oracle.propagate(w, h, dx, dy, max_time, sp, az, ec, ignitions,
-                         tile=(0 if tile == -1 else tile))
+    def run(full=0):
+        return oracle.propagate(w, h, dx, dy, max_time, sp, az, ec, ignitions,
+                                tile=(0 if tile == -1 else tile), full=full)
+    o = run()
     assert np.array_equal(res.boundary_change, o.boundaries), "boundary bits"
     t_gpu = res.arrival_times.view(np.uint32)
     t_ref = o.time.view(np.uint32)
@@ -44,8 +67,7 @@ def _check(pp, oracle, terrain, w, h, dx, dy, max_time, ignitions, tile):
                     f"ref={o.time[tuple(i)]}")
     assert np.array_equal(res.refs_x.reshape(h, w), o.refs_x)
     assert np.array_equal(res.refs_y.reshape(h, w), o.refs_y)
-    for k in ("rounds", "launches", "sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
-        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+    _check_counts(res, o, run)
     assert res.stats["burned"] == int(np.sum(o.time < FMAX))
     return res, o
 
@@ -84,12 +106,13 @@ def test_shared_memory_and_global_tiles(pp, oracle, cluster):
     s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
     res = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=-1, cluster=cluster)
     sp, az, ec = _fire(pp, sc.terrain)
-    o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
-                         sc.ignitions, tile=0)
+    def run(full=0):
+        return oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                                sc.ignitions, tile=0, full=full)
+    o = run()
     assert np.array_equal(res.arrival_times.view(np.uint32), o.time.view(np.uint32))
     assert np.array_equal(res.refs_x.reshape(sc.height, sc.width), o.refs_x)
-    for k in ("sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
-        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+    _check_counts(res, o, run, ("sweeps", "improvements") + WORK)
 
 
 @pytest.mark.parametrize("tile,cluster", [(300, 16), (300, 8), (323, 0), (300, -1), (64, -1)])
@@ -102,13 +125,17 @@ def test_wide_tiles_several_launches(pp, oracle, tile, cluster):
     s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
     res = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=tile, cluster=cluster)
     sp, az, ec = _fire(pp, sc.terrain)
-    o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
-                         sc.ignitions, tile=tile)
+    def run(full=0):
+        return oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                                sc.ignitions, tile=tile, full=full)
+    o = run()
     assert res.stats["launches"] > 4
     assert np.array_equal(res.arrival_times.view(np.uint32), o.time.view(np.uint32))
     assert np.array_equal(res.refs_x.reshape(sc.height, sc.width), o.refs_x)
-    for k in ("rounds", "launches", "sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
-        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+    mode = _check_counts(res, o, run)
+    # shared-memory clusters evaluate whole first sweeps, global-memory tiles
+    # (group mode) only the pending cells
+    assert mode == (0 if cluster > 0 else 2)
 
 
 @pytest.mark.parametrize("cluster", [1, 2])
@@ -121,14 +148,15 @@ def test_shared_memory_list_overflow(pp, oracle, cluster):
     s = _settings(pp, sc.width, sc.height, sc.dx, sc.dy, sc.max_time)
     res = pp.propagate_arrays(s, sc.terrain, sc.ignitions, tile=-1, cluster=cluster)
     sp, az, ec = _fire(pp, sc.terrain)
-    o = oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
-                         sc.ignitions, tile=0)
+    def run(full=0):
+        return oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec,
+                                sc.ignitions, tile=0, full=full)
+    o = run()
     assert res.stats["improvements"] > 2048 * cluster
     assert np.array_equal(res.arrival_times.view(np.uint32), o.time.view(np.uint32))
     assert np.array_equal(res.refs_x.reshape(sc.height, sc.width), o.refs_x)
     assert np.array_equal(res.refs_y.reshape(sc.height, sc.width), o.refs_y)
-    for k in ("sweeps", "improvements", "evaluations", "dda_steps", "gathers"):
-        assert res.stats[k] == o.stats[k], (k, res.stats[k], o.stats[k])
+    _check_counts(res, o, run, ("sweeps", "improvements") + WORK)
 
 
 def test_north_up_and_staggered_ignition_times(pp, oracle):

@@ -129,6 +129,31 @@ def test_work_skipping_equals_full_sweeps(oracle, size, kind, tile):
     assert a.stats["evaluations"] < b.stats["evaluations"]
 
 
+@pytest.mark.parametrize("size,kind,tile,north_up", [(96, 0, 31, False), (120, 1, 50, False),
+                                                     (120, 1, 19, True), (150, 1, 37, False),
+                                                     (96, 0, 0, False)])
+def test_first_sweep_skipping_equals_full_sweeps(oracle, size, kind, tile, north_up):
+    """full = 2: a launch's first sweep evaluates only the cells whose inputs
+    changed since their last evaluation (grid-wide pending bitmap, referrer
+    boxes scanned whole): same times, references and schedule as evaluating
+    every cell, with fewer evaluations when there are several tiles."""
+    sc = _scenario(size, kind, seed=5)
+    dy = -sc.dy if north_up else sc.dy
+    f, _ = oracle.burn_f64(sc.terrain)
+    sp, az, ec = (f[:, k].astype(np.float32) for k in (4, 5, 6))
+    runs = [oracle.propagate(sc.width, sc.height, sc.dx, dy, sc.max_time, sp, az, ec, sc.ignitions,
+                             tile=tile, full=m) for m in (1, 0, 2)]
+    full, skip, skip2 = runs
+    for r in (skip, skip2):
+        assert np.array_equal(r.time_raw.view(np.uint32), full.time_raw.view(np.uint32))
+        assert np.array_equal(r.refs_x, full.refs_x) and np.array_equal(r.refs_y, full.refs_y)
+        for k in ("rounds", "launches", "sweeps", "improvements"):
+            assert r.stats[k] == full.stats[k], k
+    assert skip2.stats["evaluations"] <= skip.stats["evaluations"]
+    if full.stats["launches"] > 1 and full.stats["improvements"] > 0:
+        assert skip2.stats["evaluations"] < skip.stats["evaluations"]
+
+
 def test_readme_demo_soft_pin(oracle, pp):
     """Reference demo (crates/propag/src/main.rs:12-55): 1024 x 1024 at 5 m,
     uniform NFFL 1, moistures 0.1, wind 5 m/s toward azimuth 0, flat, one

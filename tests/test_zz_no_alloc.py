@@ -69,8 +69,10 @@ def test_static_equals_engine_on_consecutive_calls(pp):
     st_b = _static(L, b)
     out_b = _outputs(kb)
 
-    # the existing entry point on the same jobs
-    eng = pp.Engine()
+    # the existing entry point on the same jobs, on a 16-CTA cluster as the
+    # fixed-scratch path runs (the same results in every mode; the work
+    # counters are those of cluster mode)
+    eng = pp.Engine(cluster=16)
     ref_a = eng.run([a])[0]
     ea = _outputs(ka)
     ref_b = eng.run([b])[0]
