@@ -231,70 +231,6 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def _device_jobs(L, dev, items):
-    """items: (width, height, dx, dy, max_time, tile, ignitions, terrain tensors).
-    Returns the jobs, their terrain pointer structs and the buffers that keep
-    them alive (terrain, fire rasters, ignitions, time, refs_x, refs_y, bits)."""
-    import torch
-    jobs, terrains, keep = [], [], []
-    for (w, h, dx, dy, max_time, tile, ignitions, t) in items:
-        n = w * h
-        fire = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
-        ign = np.array(list(ignitions), dtype=[("x", "<u4"), ("y", "<u4"), ("t", "<f4")])
-        ign_d = torch.from_numpy(np.frombuffer(ign.tobytes() or bytes(12), np.uint8).copy()).to(dev)
-        out = torch.empty(n, dtype=torch.float32, device=dev)
-        rx = torch.empty(n, dtype=torch.int16, device=dev)
-        ry = torch.empty(n, dtype=torch.int16, device=dev)
-        bnd = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
-        j = L.PropagJob()
-        j.width, j.height, j.dx, j.dy, j.max_time, j.tile = w, h, dx, dy, max_time, tile
-        j.speed_max, j.azimuth_max, j.eccentricity = (f.data_ptr() for f in fire)
-        j.ignitions, j.n_ignitions = ign_d.data_ptr(), len(ign)
-        j.time, j.refs_x, j.refs_y, j.boundaries = out.data_ptr(), rx.data_ptr(), ry.data_ptr(), bnd.data_ptr()
-        jobs.append(j)
-        terrains.append(L.PropagTerrainPtrs(*[t[k].data_ptr() for k in L.TERRAIN_FIELDS]))
-        keep.append((t, fire, ign_d, out, rx, ry, bnd))
-    return jobs, terrains, keep
-
-
-def ensemble_batch(L, dev, n_members):
-    """The ensemble on a shared 1024 x 1024 terrain: per-member wind speed and
-    direction, dead moisture offset and ignition, max_time 21600 s."""
-    import torch
-    from py_propag import scenarios as S
-    base, members = S.config2(n=n_members)
-    N = base.width * base.height
-    bt = {k: torch.from_numpy(np.ascontiguousarray(v).ravel()).to(dev) for k, v in base.terrain.items()}
-    items = []
-    for m in members:
-        t = dict(bt)
-        t["wind_speed"] = torch.full((N,), m["wind_speed"], dtype=torch.float32, device=dev)
-        t["wind_azimuth"] = torch.full((N,), m["wind_azimuth"], dtype=torch.float32, device=dev)
-        for k in ("d1hr", "d10hr", "d100hr"):
-            t[k] = bt[k] + np.float32(m["dead_offset"])
-        items.append((base.width, base.height, base.dx, base.dy, m["max_time"], 0, [m["ignition"]], t))
-    desc = (f"config2: {n_members}-member ensemble on a shared {base.width}x{base.height} terrain, "
-            f"per-member wind/moisture/ignition, max_time 21600 s")
-    return _device_jobs(L, dev, items), desc
-
-
-def uneven_batch(L, dev, n):
-    """Independent scenarios of uneven sizes: square grids log-uniform in
-    128..2048 at 5-30 m, own terrain and fuel, 1-10 ignitions, 1-12 h."""
-    import torch
-    from py_propag import scenarios as S
-    scs = S.config3(n=n)
-    items = []
-    for sc in scs:
-        t = {k: torch.from_numpy(np.ascontiguousarray(v).ravel()).to(dev) for k, v in sc.terrain.items()}
-        items.append((sc.width, sc.height, sc.dx, sc.dy, sc.max_time, 0, sc.ignitions, t))
-    cells = sum(sc.width * sc.height for sc in scs)
-    desc = (f"config3: {n} scenarios, square grids {min(s.width for s in scs)}.."
-            f"{max(s.width for s in scs)} at 5-30 m ({cells / 1e6:.1f} M cells), own terrain, "
-            f"1-10 ignitions, max_time 1-12 h")
-    return _device_jobs(L, dev, items), desc
-
-
 def serve_leg(lib, L, pp, dev, master, seconds: float, rate: float, budget_gb: float,
               check: int = 8) -> dict:
     """Serving loop: Poisson arrivals of window requests cut from a
@@ -303,6 +239,7 @@ def serve_leg(lib, L, pp, dev, master, seconds: float, rate: float, budget_gb: f
     requests is re-run alone through the plain path and compared bit for bit."""
     import torch
     from py_propag import scenarios as S
+    from py_propag.batches import device_jobs
     reqs = S.config4_requests(master["fuel_code"], seconds=seconds, rate=rate)
     H, W = master["fuel_code"].shape
     mt = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in master.items()}
@@ -319,7 +256,7 @@ def serve_leg(lib, L, pp, dev, master, seconds: float, rate: float, budget_gb: f
             t["wind_azimuth"] = torch.full((n * n,), r["wind_azimuth"], dtype=torch.float32, device=dev)
             for k in ("d1hr", "d10hr", "d100hr"):
                 t[k] = t[k] + np.float32(r["dead_offset"])
-            (jobs, terrains, kp) = _device_jobs(L, dev, [(n, n, 5.0, 5.0, r["max_time"], 0,
+            (jobs, terrains, kp) = device_jobs(L, dev, [(n, n, 5.0, 5.0, r["max_time"], 0,
                                                          [r["ignition"]], t)])
         prep.synchronize()
         return jobs[0], terrains[0], kp
@@ -501,6 +438,7 @@ def bench_b200(args):
 
     import py_propag as pp
     from py_propag import _lib as L
+    from py_propag.batches import ensemble_batch, uneven_batch
 
     rank, world, local = _rank_env()
     if world > 1:

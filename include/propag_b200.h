@@ -158,6 +158,43 @@ typedef struct PropagIgnition {
  * usable. */
 int propag_selftest_group_wait(uint32_t *status);
 
+/* The float arithmetic of time_from (crates/propag/src/propag.cu:269-294),
+ * PropagJob.arith and PropagOptions.arith.
+ *   PROPAG_ARITH_REFERENCE (0, the default): the reference's own operations as
+ *     nvcc compiles propag.cu with its default flags (crates/propag/build.rs:
+ *     48-69): CUDA's atan2f, the __cosf intrinsic, __frcp_rd, __fsqrt_rz, and
+ *     the two multiply-adds nvcc contracts (dx*dx + dy*dy and
+ *     from.time + distance * rcp).  Results are the reference kernel's.
+ *   PROPAG_ARITH_PORTABLE (1): a portable cosine and arctangent and every
+ *     operation rounded on its own, which a CPU reproduces bit for bit.
+ * The propagation's fixpoint depends on the last bit of these values, so the
+ * two give different (equally valid) arrival times in about 1 % of the cells
+ * of a heterogeneous scenario. */
+#define PROPAG_ARITH_REFERENCE 0
+#define PROPAG_ARITH_PORTABLE 1
+
+/* Element-wise views of the propagation's device arithmetic, for tests (no
+ * counterpart in the reference; host buffers, synchronous).
+ *
+ * propag_selftest_time_from: out[i] = time_from from cell (fx[i], fy[i]),
+ * burning since ftime[i], to cell (tx[i], ty[i]) with the fire
+ * (smax[i], azmax[i], ecc[i]) on a grid of pixel size dx, dy (dy < 0:
+ * north-up), in the arithmetic `arith` -- the device function the engine
+ * evaluates (crates/propag/src/propag.cu:269-294).
+ *
+ * propag_selftest_cosf_table: out[i] = __cosf(x), x the float whose bits
+ * are first_bits + i (the cosine the reference's time_from calls).
+ *
+ * propag_selftest_atan2f_table: out[(a + max_a) + (b + max_b) (2 max_a + 1)]
+ * = atan2f(a, b) for the integers |a| <= max_a, |b| <= max_b (the bearings
+ * the reference's time_from computes between cells). */
+int propag_selftest_time_from(int arith, uint64_t n, const int32_t *fx, const int32_t *fy,
+                              const float *ftime, const int32_t *tx, const int32_t *ty,
+                              const float *smax, const float *azmax, const float *ecc, float dx,
+                              float dy, float *out);
+int propag_selftest_cosf_table(uint32_t first_bits, uint64_t n, float *out);
+int propag_selftest_atan2f_table(int32_t max_a, int32_t max_b, float *out);
+
 typedef struct PropagOptions {
   int32_t tile;    /* default super-grid tile side; 0 = PROPAG_DEFAULT_TILE,
                       PROPAG_TILE_WHOLE_GRID = one tile for the whole grid */
@@ -166,6 +203,7 @@ typedef struct PropagOptions {
                       group mode with teams of at least N CTAs */
   int32_t threads; /* threads per CTA, multiple of 32, <= 512; 0 = 512 */
   int32_t device;  /* CUDA device ordinal; -1 = the current device */
+  int32_t arith;   /* PROPAG_ARITH_*, for propag_run_host (the engine's jobs carry their own) */
 } PropagOptions;
 
 typedef struct PropagStats {
@@ -205,7 +243,7 @@ typedef struct PropagJob {
   const float *eccentricity;
   const PropagIgnition *ignitions;
   uint32_t n_ignitions;
-  uint32_t pad;
+  uint32_t arith;       /* PROPAG_ARITH_*: 0 = the reference's arithmetic */
   float *time;          /* arrival time, s; FLT_MAX = not burned (post_propagate mask) */
   uint16_t *refs_x;     /* reference cell of each burned cell (0xFFFF: none) */
   uint16_t *refs_y;

@@ -22,6 +22,10 @@
 extern "C" {
 #endif
 
+/* Halo of a propagation block, in cells.  crates/propag/src/propag.rs:31
+ * (a pub const, which cbindgen emits into the reference's header) */
+#define HALO_RADIUS 1
+
 /* Affine geo transform (GDAL order).  crates/geometry/src/lib.rs:20-28 */
 typedef struct GT {
   float x0;

@@ -31,11 +31,17 @@ _lib = None
 _ref = None
 
 
+def reference_root() -> str:
+    """The reference checkout: $PROPAG_REFERENCE, else a `reference` folder
+    beside this repository."""
+    return os.environ.get("PROPAG_REFERENCE") or os.path.join(os.path.dirname(HERE), "..", "reference")
+
+
 def build(reference: str | None = None) -> None:
     """Compiles liboracle.so and, when the reference checkout exists, _ref/."""
     args = ["make", "-s", "-C", HERE, "all"]
     subprocess.run(args, check=True)
-    ref_root = reference or "/root/reference"
+    ref_root = os.path.abspath(reference or reference_root())
     if os.path.isdir(os.path.join(ref_root, "crates", "firelib-sys")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref_root}"], check=True)
 
@@ -157,7 +163,11 @@ def propagate(width: int, height: int, dx: float, dy: float, max_time: float,
     launch (block * grid_w); 0 = one tile (global Jacobi).  full: 0 = the
     engine's work skipping (whole tile in a launch's first sweep), 1 = every
     cell in every sweep, 2 = skipping in first sweeps too (grid-wide pending
-    bitmap); all three give the same results."""
+    bitmap); all three give the same results.  trig: the arithmetic of
+    time_from -- 0 portable (the engine's PROPAG_ARITH_PORTABLE), 1 libm
+    cosine/arctangent, 2 libm plus the reference's fused multiply-adds, 3 as 2
+    with the GPU's __cosf/atan2f tables (the engine's PROPAG_ARITH_REFERENCE;
+    see set_device_tables)."""
     lib = _load()
     s_arr, a_arr, e_arr = (np.ascontiguousarray(x, dtype=np.float32).ravel() for x in (speed, az, ecc))
     if time0 is None:
@@ -180,6 +190,77 @@ def propagate(width: int, height: int, dx: float, dy: float, max_time: float,
     return OracleResult(time.reshape(height, width), raw.reshape(height, width),
                         rx.reshape(height, width), ry.reshape(height, width), bits,
                         dict(zip(STAT_NAMES, (int(v) for v in stats))))
+
+
+_tables = None  # keeps the arrays given to ops_set_tables alive
+
+
+def set_device_tables(cos_tab, cos_lo: int, cos_below: float, atan_tab, max_a: int,
+                      max_b: int) -> None:
+    """Installs the GPU's __cosf values -- cos_tab[i] for the float with bits
+    cos_lo + i, and the constant cos_below for every float with smaller bits
+    -- and its atan2f values over integer pairs (|a| <= max_a, |b| <= max_b)
+    for trig = 3; cos_tab None uninstalls them."""
+    global _tables
+    lib = _load()
+    lib.ops_set_tables.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.c_float, C.c_void_p,
+                                   C.c_int, C.c_int]
+    if cos_tab is None:
+        _tables = None
+        lib.ops_set_tables(None, 0, 0, 1.0, None, -1, -1)
+        return
+    c = np.ascontiguousarray(cos_tab, dtype=np.float32)
+    a = np.ascontiguousarray(atan_tab, dtype=np.float32)
+    assert a.size == (2 * max_a + 1) * (2 * max_b + 1)
+    _tables = (c, a)
+    lib.ops_set_tables(_ptr(c), C.c_uint32(cos_lo), C.c_uint64(c.size), C.c_float(cos_below), _ptr(a),
+                       int(max_a), int(max_b))
+
+
+# Range of the trig = 3 tables.  The cosine's argument is |bearing -
+# azimuth_max|, in [0, 3 pi] (bearings in [-pi, pi], azimuths in [0, 2 pi));
+# the bearings are atan2f of cell offsets.
+COS_TABLE_LO = 0x35800000  # 2^-20: below it __cosf must be one constant (checked)
+COS_TABLE_HI = 0x41180000  # 9.5 > 3 pi
+
+
+def install_device_tables(lib, max_offset: int = 4095) -> None:
+    """Builds the trig = 3 tables from the device (libpropag's
+    propag_selftest_cosf_table / propag_selftest_atan2f_table, given as the
+    ctypes library `lib`) and installs them: __cosf of every float with bits
+    in [lo, COS_TABLE_HI), lo = COS_TABLE_LO unless the device's values below
+    it are not all one constant, and atan2f of every integer pair within
+    max_offset (grids up to max_offset + 1 cells per side)."""
+    chunk = 1 << 26
+    below = None
+    lo = COS_TABLE_LO
+    buf = np.empty(chunk, np.float32)
+    for o in range(0, COS_TABLE_LO, chunk):
+        m = min(chunk, COS_TABLE_LO - o)
+        if lib.propag_selftest_cosf_table(o, m, buf.ctypes.data) != 0:
+            raise RuntimeError("propag_selftest_cosf_table failed")
+        t = buf[:m]
+        if below is None:
+            below = t[0]
+        bad = np.nonzero(t != below)[0]
+        if bad.size:  # not constant there: the table starts at the first other value
+            lo = o + int(bad[0])
+            break
+    tab = np.empty(COS_TABLE_HI - lo, np.float32)
+    if lib.propag_selftest_cosf_table(lo, tab.size, tab.ctypes.data) != 0:
+        raise RuntimeError("propag_selftest_cosf_table failed")
+    w = 2 * max_offset + 1
+    atan = np.empty(w * w, np.float32)
+    if lib.propag_selftest_atan2f_table(max_offset, max_offset, atan.ctypes.data) != 0:
+        raise RuntimeError("propag_selftest_atan2f_table failed")
+    set_device_tables(tab, lo, float(below), atan, max_offset, max_offset)
+
+
+def table_misses() -> int:
+    """Look-ups outside the trig = 3 tables since they were installed."""
+    lib = _load()
+    lib.ops_table_misses.restype = C.c_int64
+    return int(lib.ops_table_misses())
 
 
 def time_from_batch(dx, dy, fx, fy, ftime, tx, ty, smax, azmax, ecc, trig=0):

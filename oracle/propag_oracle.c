@@ -44,9 +44,15 @@
  *
  * Intrinsics: __frcp_rd and __fsqrt_rz are emulated exactly (round-down
  * reciprocal, round-toward-zero square root).  The cosine and arctangent are
- * the portable float routines below (trig = 0), which the device kernel
- * evaluates with the same float operations, or libm's cosf/atan2f (trig = 1).
- * Build with -ffp-contract=off: every float operation is rounded on its own.
+ * the portable float routines below (trig = 0), which the device kernel's
+ * portable arithmetic evaluates with the same float operations, or libm's
+ * cosf/atan2f (trig = 1).  trig = 2 follows the reference kernel as nvcc
+ * compiles it: libm's cosf/atan2f standing in for CUDA's __cosf/atan2f (which
+ * a CPU cannot reproduce bit for bit) and the two multiply-adds of time_from
+ * fused; trig = 3 also takes the cosine and arctangent from tables of the
+ * GPU's values (ops_set_tables), so that it follows the reference kernel's
+ * arithmetic exactly.  Build with -ffp-contract=off: every other float
+ * operation is rounded on its own.
  */
 #include <float.h>
 #include <math.h>
@@ -160,9 +166,64 @@ float pg_atan2f(float y, float x) {
   return a;
 }
 
+/* 0: portable cosine/arctangent above; 1: libm's cosf/atan2f; 2: libm's
+ * cosf/atan2f and the reference's contracted sums (see time_from); 3: as 2,
+ * with the cosine and arctangent looked up in tables of the GPU's own
+ * __cosf and atan2f values (ops_set_tables), which makes this restatement
+ * follow the reference kernel's arithmetic bit for bit. */
 static int g_trig = 0;
-static inline float t_cos(float x) { return g_trig ? cosf(x) : pg_cosf(x); }
-static inline float t_atan2(float y, float x) { return g_trig ? atan2f(y, x) : pg_atan2f(y, x); }
+
+/* trig = 3 tables: cos_tab[b - cos_lo] = __cosf(x) for the float x with bits
+ * b in [cos_lo, cos_lo + cos_n), and __cosf(x) = cos_below for the bits below
+ * cos_lo (the angles are non-negative; the caller checked that the GPU's
+ * values are that constant there); atan_tab[(a + ma) + (b + mb) (2 ma + 1)]
+ * = atan2f(a, b) for integers |a| <= ma, |b| <= mb.  A look-up outside a
+ * table counts a miss and falls back to libm. */
+static const float *g_cos_tab = NULL;
+static uint64_t g_cos_n = 0;
+static uint32_t g_cos_lo = 0;
+static float g_cos_below = 1.0f;
+static const float *g_atan_tab = NULL;
+static int g_atan_ma = -1, g_atan_mb = -1;
+static int64_t g_table_misses = 0;
+
+void ops_set_tables(const float *cos_tab, uint32_t cos_lo, uint64_t cos_n, float cos_below,
+                    const float *atan_tab, int ma, int mb) {
+  g_cos_tab = cos_tab;
+  g_cos_lo = cos_lo;
+  g_cos_n = cos_tab ? cos_n : 0;
+  g_cos_below = cos_below;
+  g_atan_tab = atan_tab;
+  g_atan_ma = atan_tab ? ma : -1;
+  g_atan_mb = atan_tab ? mb : -1;
+  g_table_misses = 0;
+}
+
+int64_t ops_table_misses(void) { return __atomic_load_n(&g_table_misses, __ATOMIC_RELAXED); }
+
+static inline float t_cos(float x) {
+  if (g_trig == 3) {
+    uint32_t b;
+    memcpy(&b, &x, sizeof b);
+    if (g_cos_tab && b < g_cos_lo) return g_cos_below;
+    if (b >= g_cos_lo && (uint64_t)(b - g_cos_lo) < g_cos_n) return g_cos_tab[b - g_cos_lo];
+    __atomic_fetch_add(&g_table_misses, 1, __ATOMIC_RELAXED);
+    return cosf(x);
+  }
+  return g_trig ? cosf(x) : pg_cosf(x);
+}
+static inline float t_atan2(float y, float x) {
+  if (g_trig == 3) {
+    /* the arguments are cell offsets: integers */
+    const int a = (int)y, b = (int)x;
+    if ((float)a == y && (float)b == x && a >= -g_atan_ma && a <= g_atan_ma && b >= -g_atan_mb &&
+        b <= g_atan_mb)
+      return g_atan_tab[(int64_t)(a + g_atan_ma) + (int64_t)(b + g_atan_mb) * (2 * g_atan_ma + 1)];
+    __atomic_fetch_add(&g_table_misses, 1, __ATOMIC_RELAXED);
+    return atan2f(y, x);
+  }
+  return g_trig ? atan2f(y, x) : pg_atan2f(y, x);
+}
 
 /* ---- state ---------------------------------------------------------------- */
 
@@ -183,7 +244,12 @@ typedef struct {
 static inline int is_boundary(const uint32_t *b, int64_t ix) { return (b[ix >> 5] >> (ix & 31)) & 1u; }
 
 /* time_from, propag.cu:269-294.  The `1.0` literals make the reference
- * evaluate denom and factor in double; that is kept. */
+ * evaluate denom and factor in double; that is kept.  With g_trig >= 2 the two
+ * sums that nvcc contracts by default (the reference is built without
+ * -fmad=false, crates/propag/build.rs:48-69) are fused multiply-adds:
+ * dx*dx + dy*dy -> fmaf(dx, dx, dy*dy) and from.time + distance * rcp ->
+ * fmaf(distance, rcp, from.time); trig 0 and 1 round every operation on its
+ * own. */
 static inline float time_from(const world_t *w, int fx, int fy, float ftime, int tx, int ty,
                               float smax, float azmax, float ecc) {
   const ops_settings_t *s = w->s;
@@ -198,6 +264,10 @@ static inline float time_from(const world_t *w, int fx, int fy, float ftime, int
   float speed = smax * factor;
   float dx = (float)(fx - tx) * s->dx;
   float dy = (float)(fy - ty) * s->dy;
+  if (g_trig >= 2) {
+    const float distance = sqrt_rz(fmaf(dx, dx, dy * dy));
+    return fmaf(distance, rcp_rd(speed), ftime);
+  }
   float dx2 = dx * dx;
   float dy2 = dy * dy;
   float distance = sqrt_rz(dx2 + dy2);
@@ -224,7 +294,7 @@ static int line_blocked(const world_t *w, int fx, int fy, int tx, int ty, int64_
       int vx = sx > 0 ? cx <= tx : cx >= tx;
       int vy = sy > 0 ? cy <= ty : cy >= ty;
       if (!(vx && vy)) return 0;
-      if (fabsf(tmx - tmy) < 1e-9f) {
+      if ((double)fabsf(tmx - tmy) < 1e-9) {
         cx += sx;
         cy += sy;
         tmx += ddx;
@@ -651,7 +721,7 @@ int64_t ops_dda_cells(int fx, int fy, int tx, int ty, int32_t *out, int64_t max_
       int vx = sx > 0 ? cx <= tx : cx >= tx;
       int vy = sy > 0 ? cy <= ty : cy >= ty;
       if (!(vx && vy)) break;
-      if (fabsf(tmx - tmy) < 1e-9f) {
+      if ((double)fabsf(tmx - tmy) < 1e-9) {
         cx += sx;
         cy += sy;
         tmx += ddx;

@@ -40,6 +40,14 @@ cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *sl
 cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n);
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
                         StatsDev *stats, cudaStream_t stream);
+// selftest.cu
+cudaError_t launch_time_from(bool refm, uint64_t n, const int32_t *fx, const int32_t *fy,
+                             const float *ftime, const int32_t *tx, const int32_t *ty,
+                             const float *smax, const float *azmax, const float *ecc, float gdx,
+                             float gdy, bool north_up, float *out, cudaStream_t stream);
+cudaError_t launch_cosf_table(uint32_t first, uint64_t n, float *out, cudaStream_t stream);
+cudaError_t launch_atan2f_table(int32_t ma, int32_t mb, int32_t b0, int32_t nb, float *out,
+                                cudaStream_t stream);
 
 namespace {
 
@@ -232,6 +240,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
       return fail(PROPAG_ERR_INVALID, "job " + std::to_string(i) + ": null ignitions");
     if (!(j.dx != 0.0f) || !(j.dy != 0.0f) || !std::isfinite(j.dx) || !std::isfinite(j.dy))
       return fail(PROPAG_ERR_INVALID, "job " + std::to_string(i) + ": invalid pixel size");
+    if (j.arith != PROPAG_ARITH_REFERENCE && j.arith != PROPAG_ARITH_PORTABLE)
+      return fail(PROPAG_ERR_INVALID, "job " + std::to_string(i) + ": arith must be PROPAG_ARITH_REFERENCE or PROPAG_ARITH_PORTABLE");
     const uint64_t N = (uint64_t)j.width * j.height;
     const uint64_t words = (N + 31) / 32;
     int T = j.tile ? j.tile : e->default_tile;
@@ -246,6 +256,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     d.TX = (int)((j.width + T - 1) / T);
     d.TY = (int)((j.height + T - 1) / T);
     d.north_up = j.dy < 0 ? 1 : 0;
+    d.refm = j.arith == PROPAG_ARITH_REFERENCE ? 1 : 0;
     d.speed = j.speed_max;
     d.az = j.azimuth_max;
     d.ecc = j.eccentricity;
@@ -783,6 +794,8 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   if (j.n_ignitions && !j.ignitions) return fail(PROPAG_ERR_INVALID, "null ignitions");
   if (!(j.dx != 0.0f) || !(j.dy != 0.0f) || !std::isfinite(j.dx) || !std::isfinite(j.dy))
     return fail(PROPAG_ERR_INVALID, "invalid pixel size");
+  if (j.arith != PROPAG_ARITH_REFERENCE && j.arith != PROPAG_ARITH_PORTABLE)
+    return fail(PROPAG_ERR_INVALID, "arith must be PROPAG_ARITH_REFERENCE or PROPAG_ARITH_PORTABLE");
   int T = j.tile ? j.tile : PROPAG_DEFAULT_TILE;
   if (T == PROPAG_TILE_WHOLE_GRID || T <= 0) T = (int)std::max(j.width, j.height);
   const int tw = std::min<int>(T, (int)j.width), th = std::min<int>(T, (int)j.height);
@@ -822,6 +835,7 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   d.TX = (int)((j.width + T - 1) / T);
   d.TY = (int)((j.height + T - 1) / T);
   d.north_up = j.dy < 0 ? 1 : 0;
+  d.refm = j.arith == PROPAG_ARITH_REFERENCE ? 1 : 0;
   d.smem_tile = exact ? kSmemTileExact : kSmemTileCoarse;
   d.speed = j.speed_max;
   d.az = j.azimuth_max;
@@ -1139,6 +1153,7 @@ extern "C" int propag_run_host(const Settings *settings, const PropagTerrainPtrs
   job.eccentricity = d_ecc;
   job.ignitions = d_ign;
   job.n_ignitions = (uint32_t)n_ignitions;
+  job.arith = (uint32_t)o.arith;
   job.time = d_time;
   job.refs_x = d_rx;
   job.refs_y = d_ry;
@@ -1178,6 +1193,65 @@ extern "C" int propag_write_geotiff(const GeoReference *g, const float *time, co
   if (!g || !time || !path) return fail(PROPAG_ERR_INVALID, "null argument");
   std::string err;
   if (!write_geotiff_f32(path, *g, time, err)) return fail(PROPAG_ERR_INVALID, err);
+  return PROPAG_OK;
+}
+
+// ======================================================= self-tests =======
+extern "C" int propag_selftest_time_from(int arith, uint64_t n, const int32_t *fx, const int32_t *fy,
+                                         const float *ftime, const int32_t *tx, const int32_t *ty,
+                                         const float *smax, const float *azmax, const float *ecc,
+                                         float dx, float dy, float *out) {
+  int rc = ensure_device(-1, nullptr);
+  if (rc) return rc;
+  if (arith != PROPAG_ARITH_REFERENCE && arith != PROPAG_ARITH_PORTABLE)
+    return fail(PROPAG_ERR_INVALID, "arith must be PROPAG_ARITH_REFERENCE or PROPAG_ARITH_PORTABLE");
+  if (n == 0) return PROPAG_OK;
+  if (!fx || !fy || !ftime || !tx || !ty || !smax || !azmax || !ecc || !out)
+    return fail(PROPAG_ERR_INVALID, "null argument");
+  DevBuf b;
+  const size_t a = align_up(n * 4, 256);
+  CK(b.reserve(10 * a, nullptr));
+  const void *src[9] = {fx, fy, ftime, tx, ty, smax, azmax, ecc};
+  for (int k = 0; k < 8; ++k) CK(cudaMemcpy(b.at<char>(k * a), src[k], n * 4, cudaMemcpyHostToDevice));
+  CK(launch_time_from(arith == PROPAG_ARITH_REFERENCE, n, b.at<int32_t>(0), b.at<int32_t>(a),
+                      b.at<float>(2 * a), b.at<int32_t>(3 * a), b.at<int32_t>(4 * a),
+                      b.at<float>(5 * a), b.at<float>(6 * a), b.at<float>(7 * a), dx, dy, dy < 0,
+                      b.at<float>(8 * a), nullptr));
+  CK(cudaMemcpy(out, b.at<float>(8 * a), n * 4, cudaMemcpyDeviceToHost));
+  return PROPAG_OK;
+}
+
+extern "C" int propag_selftest_cosf_table(uint32_t first_bits, uint64_t n, float *out) {
+  int rc = ensure_device(-1, nullptr);
+  if (rc) return rc;
+  if (n == 0) return PROPAG_OK;
+  if (!out) return fail(PROPAG_ERR_INVALID, "null output");
+  if ((uint64_t)first_bits + n > (1ull << 32)) return fail(PROPAG_ERR_INVALID, "bit range past 2^32");
+  const uint64_t chunk = 1ull << 26;  // 256 MB of floats per pass
+  DevBuf b;
+  CK(b.reserve(std::min(n, chunk) * 4, nullptr));
+  for (uint64_t o = 0; o < n; o += chunk) {
+    const uint64_t m = std::min(chunk, n - o);
+    CK(launch_cosf_table(first_bits + (uint32_t)o, m, b.at<float>(0), nullptr));
+    CK(cudaMemcpy(out + o, b.at<float>(0), m * 4, cudaMemcpyDeviceToHost));
+  }
+  return PROPAG_OK;
+}
+
+extern "C" int propag_selftest_atan2f_table(int32_t max_a, int32_t max_b, float *out) {
+  int rc = ensure_device(-1, nullptr);
+  if (rc) return rc;
+  if (max_a < 0 || max_b < 0 || max_a > 65535 || max_b > 65535 || !out)
+    return fail(PROPAG_ERR_INVALID, "table half-widths must be 0..65535, output non-null");
+  const int64_t w = 2 * (int64_t)max_a + 1, h = 2 * (int64_t)max_b + 1;
+  const int32_t rows = (int32_t)std::max<int64_t>(1, std::min<int64_t>(h, (1 << 26) / w));
+  DevBuf b;
+  CK(b.reserve((size_t)(w * rows * 4), nullptr));
+  for (int32_t r0 = 0; r0 < h; r0 += rows) {
+    const int32_t nb = (int32_t)std::min<int64_t>(rows, h - r0);
+    CK(launch_atan2f_table(max_a, max_b, r0, nb, b.at<float>(0), nullptr));
+    CK(cudaMemcpy(out + (size_t)r0 * w, b.at<float>(0), (size_t)(w * nb * 4), cudaMemcpyDeviceToHost));
+  }
   return PROPAG_OK;
 }
 

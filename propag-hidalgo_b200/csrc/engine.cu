@@ -73,33 +73,33 @@ struct DirConst {
 };
 
 __device__ __forceinline__ void dir_consts(const JobDev &j, DirConst &d) {
-  const bool nu = j.north_up != 0;
+  const bool nu = j.north_up != 0, refm = j.refm != 0;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int kk = k < 4 ? k : k + 1;
     const int di = kk % 3 - 1, dj = kk / 3 - 1;
-    d.bearing[k] = bearing(di, dj, 0, 0, nu);
-    d.dist[k] = cell_distance(di, dj, j.gdx, j.gdy);
+    d.bearing[k] = bearing(di, dj, 0, 0, nu, refm);
+    d.dist[k] = cell_distance(di, dj, j.gdx, j.gdy, refm);
   }
 }
 
-// Travel time of the direct spread from a cell with fire f to the cell it is
-// neighbour k of: the distance over the elliptical speed along that bearing,
-// the operations of step_time without the start time, so that
-// ftime + travel_time(...) is bit-identical to step_time(ftime, ...).
-__device__ __forceinline__ float travel_time(const DirConst &dc, int k, const Fire &f) {
-  return __fmul_rn(dc.dist[k], __frcp_rd(__fmul_rn(f.speed_max, spread_factor(dc.bearing[k], f))));
+// Round-down reciprocal of the elliptical speed of a cell with fire f toward
+// the cell it is neighbour k of, so that step_time(ftime, dc.dist[k], inv)
+// is bit-identical to time_from(neighbour -> cell).
+__device__ __forceinline__ float dir_inv_speed(const DirConst &dc, int k, const Fire &f, bool refm) {
+  return inv_speed(dc.bearing[k], f, refm);
 }
 
 // ---------------------------------------------------------------- prep ----
 // Boundary bits (find_boundaries) packed with a warp ballot, plus the initial
 // state: time = FLT_MAX, no reference, empty referrer boxes; and the
-// direct-spread travel times toward the 8 neighbours (when the job has them).
+// reciprocal direct-spread speeds toward the 8 neighbours (when the job has them).
 __global__ void __launch_bounds__(256) prep_kernel(const JobDev *__restrict__ jobs) {
   const JobDev j = jobs[blockIdx.y];
   __shared__ DirConst dc;
   if (threadIdx.x == 0) dir_consts(j, dc);
   __syncthreads();
+  const bool refm = j.refm != 0;
   const int64_t N = (int64_t)j.W * j.H;
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(256) prep_kernel(const JobDev *__restrict__ jo
       }
       if (j.tt && me.speed_max != 0.0f) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) j.tt[k * j.tt_plane + i] = travel_time(dc, k, me);
+        for (int k = 0; k < 8; ++k) j.tt[k * j.tt_plane + i] = dir_inv_speed(dc, k, me, refm);
       }
       j.time[i] = FLT_MAX;
       j.refs[i] = kNoRef;
@@ -264,8 +264,10 @@ __device__ __forceinline__ Best evaluate_coop(const JobDev &j, const DirConst &d
   uint32_t oref = 0, steps = 0;
   bool walked = false;
   if (act) {
-    const float ntime = j.tt ? __fadd_rn(nt, tt) : __fadd_rn(nt, travel_time(dc, k, f));
-    cand = time_from(ref_x(nr), ref_y(nr), rt, x, y, f, j.gdx, j.gdy, j.north_up != 0);
+    const bool refm = j.refm != 0;
+    const float ntime =
+        step_time(nt, dc.dist[k], j.tt ? tt : dir_inv_speed(dc, k, f, refm), refm);
+    cand = time_from(ref_x(nr), ref_y(nr), rt, x, y, f, j.gdx, j.gdy, j.north_up != 0, refm);
     offer = ntime;
     oref = pack_ref(nx, ny);
     if (cand < ntime) {

@@ -13,6 +13,7 @@ struct JobDev {
   int32_t TX, TY;  // tiles per axis
   int32_t north_up;
   int32_t smem_tile;  // kSmemTile*: where tile launches keep the tile's state
+  int32_t refm;       // 1: the reference's arithmetic in time_from, 0: portable
   const float *speed, *az, *ecc;
   float *time;         // state, becomes the output after the post pass
   uint32_t *refs;      // state: packed x | y << 16
@@ -25,9 +26,10 @@ struct JobDev {
   uint32_t pad;
   uint16_t *out_rx, *out_ry;
   uint32_t *out_bnd;   // caller's boundary output (may alias bnd)
-  // Direct-spread travel time of every cell toward each of its 8 neighbours
-  // (plane k: toward the cell whose neighbour k it is), written by the prep
-  // pass; null = computed per evaluation instead.  Plane stride tt_plane.
+  // Round-down reciprocal of every cell's elliptical speed toward each of its
+  // 8 neighbours (plane k: toward the cell whose neighbour k it is), written
+  // by the prep pass; null = computed per evaluation instead.  Plane stride
+  // tt_plane.
   float *tt;
   int64_t tt_plane;
   // Second copy of the state for global-memory tiles (sweeps alternate

@@ -3,7 +3,9 @@
 // Everything here is written with explicitly rounded operations
 // (__fadd_rn, __fmul_rn, __fmaf_rn, ...) so that the compiler can neither
 // contract nor reorder them: the result of every cell evaluation is a fixed
-// sequence of IEEE operations, the same one the CPU oracle performs.
+// sequence of operations, chosen per scenario between the reference's own
+// (CUDA's atan2f and __cosf, nvcc's contracted multiply-adds) and a portable
+// IEEE sequence that a CPU reproduces (see time_from).
 //
 // Semantics follow the reference kernel (paths relative to the reference
 // project):
@@ -96,38 +98,57 @@ __device__ __forceinline__ float pg_atan2f(float y, float x) {
 // the elliptical speed of `fire` along the bearing from -> to.  The reference
 // writes `1.0 - ...` with double literals, so denom and factor are formed in
 // double and rounded to float; __frcp_rd / __fsqrt_rz as in the reference.
+//
+// Two arithmetics (`refm`, uniform per scenario):
+//   reference (refm = true, the default): the reference's own operations as
+//     nvcc compiles propag.cu with its default flags -- CUDA's atan2f and the
+//     __cosf intrinsic, and the two sums nvcc contracts into multiply-adds,
+//     dx*dx + dy*dy -> fma(dx, dx, dy*dy) and from.time + distance * rcp ->
+//     fma(distance, rcp, from.time).  A test compiles the reference's
+//     time_from from its source and checks these bits against it.
+//   portable (refm = false): the float cosine/arctangent above and every
+//     operation rounded on its own, which a CPU reproduces bit for bit (the
+//     CPU restatement checks the whole propagation schedule against it).
 struct Fire {
   float speed_max, azimuth_max, eccentricity;
 };
 
-__device__ __forceinline__ float spread_factor(float azimuth, const Fire &f) {
+__device__ __forceinline__ float spread_factor(float azimuth, const Fire &f, bool refm) {
   const float angle = fabsf(__fsub_rn(azimuth, f.azimuth_max));
-  const float p = __fmul_rn(f.eccentricity, pg_cosf(angle));
+  const float p = __fmul_rn(f.eccentricity, refm ? __cosf(angle) : pg_cosf(angle));
   const float denom = __double2float_rn(__dsub_rn(1.0, (double)p));
   const double one_minus_e = __dsub_rn(1.0, (double)f.eccentricity);
   return __double2float_rn(__dmul_rn(one_minus_e, (double)__frcp_rd(denom)));
 }
 
-__device__ __forceinline__ float step_time(float ftime, float distance, float speed) {
-  return __fadd_rn(ftime, __fmul_rn(distance, __frcp_rd(speed)));
+// Round-down reciprocal of the elliptical speed along `azimuth`.
+__device__ __forceinline__ float inv_speed(float azimuth, const Fire &f, bool refm) {
+  return __frcp_rd(__fmul_rn(f.speed_max, spread_factor(azimuth, f, refm)));
 }
 
-__device__ __forceinline__ float cell_distance(int ddx, int ddy, float gdx, float gdy) {
+// from.time + distance * __frcp_rd(speed), given the reciprocal.
+__device__ __forceinline__ float step_time(float ftime, float distance, float inv, bool refm) {
+  return refm ? __fmaf_rn(distance, inv, ftime) : __fadd_rn(ftime, __fmul_rn(distance, inv));
+}
+
+__device__ __forceinline__ float cell_distance(int ddx, int ddy, float gdx, float gdy, bool refm) {
   const float dx = __fmul_rn((float)ddx, gdx);
   const float dy = __fmul_rn((float)ddy, gdy);
-  return __fsqrt_rz(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+  return __fsqrt_rz(refm ? __fmaf_rn(dx, dx, __fmul_rn(dy, dy))
+                         : __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
 }
 
-__device__ __forceinline__ float bearing(int fx, int fy, int tx, int ty, bool north_up) {
-  return north_up ? pg_atan2f((float)(tx - fx), (float)(fy - ty))
-                  : pg_atan2f((float)(tx - fx), (float)(ty - fy));
+__device__ __forceinline__ float bearing(int fx, int fy, int tx, int ty, bool north_up, bool refm) {
+  const float y = (float)(tx - fx);
+  const float x = north_up ? (float)(fy - ty) : (float)(ty - fy);
+  return refm ? atan2f(y, x) : pg_atan2f(y, x);
 }
 
 __device__ __forceinline__ float time_from(int fx, int fy, float ftime, int tx, int ty,
-                                           const Fire &f, float gdx, float gdy, bool north_up) {
-  const float factor = spread_factor(bearing(fx, fy, tx, ty, north_up), f);
-  const float speed = __fmul_rn(f.speed_max, factor);
-  return step_time(ftime, cell_distance(fx - tx, fy - ty, gdx, gdy), speed);
+                                           const Fire &f, float gdx, float gdy, bool north_up,
+                                           bool refm) {
+  const float inv = inv_speed(bearing(fx, fy, tx, ty, north_up, refm), f, refm);
+  return step_time(ftime, cell_distance(fx - tx, fy - ty, gdx, gdy, refm), inv, refm);
 }
 
 // ---- DDA line-of-sight walk (propag.h:91-135) ------------------------------
@@ -158,7 +179,7 @@ __device__ __forceinline__ bool line_blocked(const uint32_t *__restrict__ bnd, i
       const bool vx = sx > 0 ? cx <= tx : cx >= tx;
       const bool vy = sy > 0 ? cy <= ty : cy >= ty;
       if (!(vx && vy)) return false;
-      if (fabsf(__fsub_rn(tmx, tmy)) < 1e-9f) {
+      if ((double)fabsf(__fsub_rn(tmx, tmy)) < 1e-9) {  // a double comparison, propag.h:122
         cx += sx;
         cy += sy;
         tmx = __fadd_rn(tmx, ddx);

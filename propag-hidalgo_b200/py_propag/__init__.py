@@ -303,14 +303,22 @@ def _ignition_array(ignitions):
     return arr, len(items)
 
 
-def _options(tile, cluster=0, threads=0, device=-1):
-    return L.PropagOptions(int(tile or 0), int(cluster or 0), int(threads or 0), int(device))
+ARITH_REFERENCE = L.PROPAG_ARITH_REFERENCE
+ARITH_PORTABLE = L.PROPAG_ARITH_PORTABLE
+
+
+def _options(tile, cluster=0, threads=0, device=-1, arith=ARITH_REFERENCE):
+    return L.PropagOptions(int(tile or 0), int(cluster or 0), int(threads or 0), int(device),
+                           int(arith))
 
 
 def propagate_arrays(settings: PySettings, terrain: dict, ignitions, *, tile=None, cluster=0,
-                     threads=0) -> PyPropagResults:
+                     threads=0, arith=ARITH_REFERENCE) -> PyPropagResults:
     """Fire behaviour + propagation for one grid, no files.  ignitions:
-    iterable of (x, y, t) cells or the output of ``rasterize_ignitions``."""
+    iterable of (x, y, t) cells or the output of ``rasterize_ignitions``.
+    arith: the float arithmetic of the propagation's time_from --
+    ARITH_REFERENCE (the reference kernel's operations, the default) or
+    ARITH_PORTABLE (operations a CPU reproduces bit for bit)."""
     lib = L.lib()
     g = settings.geo_ref
     n = g.width * g.height
@@ -321,7 +329,7 @@ def propagate_arrays(settings: PySettings, terrain: dict, ignitions, *, tile=Non
     ry = np.empty(n, np.uint16)
     bnd = np.empty((n + 31) // 32, np.uint32)
     st = L.PropagStats()
-    opt = _options(tile, cluster, threads)
+    opt = _options(tile, cluster, threads, arith=arith)
     s = settings.inner
     rc = lib.propag_run_host(C.byref(s), C.byref(ptrs), ign, n_ign, C.byref(opt),
                              time.ctypes.data, rx.ctypes.data, ry.ctypes.data, bnd.ctypes.data,

@@ -21,6 +21,8 @@ PROPAG_ERR_OOM = -5
 PROPAG_DEFAULT_TILE = 323
 PROPAG_TILE_WHOLE_GRID = -1
 PROPAG_CLUSTER_GROUPS = -1  # PropagOptions.cluster: teams of CTAs over the whole device
+PROPAG_ARITH_REFERENCE = 0  # time_from with the reference's operations (CUDA atan2f, __cosf, contracted)
+PROPAG_ARITH_PORTABLE = 1   # time_from with portable operations a CPU reproduces bit for bit
 SERVER_DEFAULT_BYTES_PER_CELL = 96  # a request's device memory when submit gets 0
 
 
@@ -105,7 +107,8 @@ class PropagIgnition(C.Structure):
 
 
 class PropagOptions(C.Structure):
-    _fields_ = [("tile", C.c_int32), ("cluster", C.c_int32), ("threads", C.c_int32), ("device", C.c_int32)]
+    _fields_ = [("tile", C.c_int32), ("cluster", C.c_int32), ("threads", C.c_int32), ("device", C.c_int32),
+                ("arith", C.c_int32)]
 
 
 PROPAG_STATIC_MAX_CELLS = 1 << 20  # propag_run_device_static's fixed scratch
@@ -132,7 +135,7 @@ class PropagJob(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("dx", C.c_float), ("dy", C.c_float),
                 ("max_time", C.c_float), ("tile", C.c_int32),
                 ("speed_max", C.c_void_p), ("azimuth_max", C.c_void_p), ("eccentricity", C.c_void_p),
-                ("ignitions", C.c_void_p), ("n_ignitions", C.c_uint32), ("pad", C.c_uint32),
+                ("ignitions", C.c_void_p), ("n_ignitions", C.c_uint32), ("arith", C.c_uint32),
                 ("time", C.c_void_p), ("refs_x", C.c_void_p), ("refs_y", C.c_void_p),
                 ("boundaries", C.c_void_p)]
 
@@ -185,6 +188,10 @@ SIGNATURES = {
                                     C.POINTER(PropagStats)]),
     "propag_engine_last_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float * 3)]),
     "propag_selftest_group_wait": (C.c_int, [C.POINTER(C.c_uint32)]),
+    "propag_selftest_time_from": (C.c_int, [C.c_int, C.c_uint64] + [C.c_void_p] * 8 +
+                                  [C.c_float, C.c_float, C.c_void_p]),
+    "propag_selftest_cosf_table": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p]),
+    "propag_selftest_atan2f_table": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p]),
     "propag_slope_aspect_device": (C.c_int, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "propag_dmoist_device": (C.c_int, [C.c_uint64, C.c_int, C.c_int, C.POINTER(PropagWeatherPtrs),

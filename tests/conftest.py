@@ -30,6 +30,25 @@ def oracle():
     return O
 
 
+def trig_for(arith: int) -> int:
+    """The oracle's trig mode that follows the engine's arithmetic `arith`:
+    3 (the device's __cosf/atan2f tables) for PROPAG_ARITH_REFERENCE, 0 for
+    PROPAG_ARITH_PORTABLE."""
+    return 3 if arith == 0 else 0
+
+
+@pytest.fixture(scope="session")
+def ref_oracle():
+    """The oracle with the device's __cosf and atan2f values installed (use
+    trig=3 for PROPAG_ARITH_REFERENCE results; grids up to 4096 cells a side)."""
+    from oracle import oracle
+    from py_propag import _lib as L
+    oracle._load()
+    oracle.install_device_tables(L.lib(), 4095)
+    yield oracle
+    oracle.set_device_tables(None, 0, 1.0, None, 0, 0)
+
+
 @pytest.fixture(scope="session")
 def pp():
     import py_propag
