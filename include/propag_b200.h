@@ -163,7 +163,7 @@ int propag_selftest_group_wait(uint32_t *status);
  *   PROPAG_ARITH_REFERENCE (0, the default): the reference's own operations as
  *     nvcc compiles propag.cu with its default flags (crates/propag/build.rs:
  *     48-69): CUDA's atan2f, the __cosf intrinsic, __frcp_rd, __fsqrt_rz, and
- *     the two multiply-adds nvcc contracts (dx*dx + dy*dy and
+ *     the three multiply-adds nvcc contracts (1 - e*cos, dx*dx + dy*dy and
  *     from.time + distance * rcp).  Results are the reference kernel's.
  *   PROPAG_ARITH_PORTABLE (1): a portable cosine and arctangent and every
  *     operation rounded on its own, which a CPU reproduces bit for bit.
@@ -381,10 +381,24 @@ int propag_autotune(const PropagJob *jobs, const PropagTerrainPtrs *terrains, ui
  * capture.
  *
  * Stream-ordered: returns once the work is enqueued on `stream`, unless stats
- * is non-NULL, in which case it synchronises the stream and fills *stats.
+ * is non-NULL, in which case it synchronises the stream and fills *stats
+ * (and fails with PROPAG_ERR_TIMEOUT if the job hit the sweep limit); a
+ * caller that passes no stats reads the job's outcome with
+ * propag_static_last_status before its next call.
  * The job's pointers are device pointers, as in propag_engine_run. */
 #define PROPAG_STATIC_MAX_CELLS (1u << 20)
 int propag_run_device_static(const PropagJob *job, void *stream, PropagStats *stats);
+
+/* Outcome of the last propag_run_device_static on the current device, for
+ * callers that ran it without `stats` (stream-ordered, no synchronisation):
+ * waits for `stream` (the stream of that call), copies the job's statistics
+ * out of the fixed scratch into *stats (may be NULL) and returns
+ * PROPAG_ERR_TIMEOUT when the job ended on a device-side error (the sweep
+ * limit), else PROPAG_OK.  Call it before the next propag_run_device_static
+ * on the device, which clears the statistics.  Allocates nothing.  No
+ * counterpart in the reference (its propagation reports errors synchronously,
+ * crates/propag/src/propag.rs:323-574). */
+int propag_static_last_status(void *stream, PropagStats *stats);
 
 /* Plain drop-in over host buffers for one grid: fire behaviour (3 fields),
  * boundaries, propagation and post mask, like propagate()

@@ -6,7 +6,7 @@ atan2f and __cosf and is compiled with nvcc's default multiply-add
 contraction (crates/propag/build.rs:48-69).  The CPU restatement runs in
 three modes (oracle/propag_oracle.c): trig 0 = the portable cosine and
 arctangent, every operation rounded on its own; trig 1 = libm's cosf/atan2f;
-trig 2 = libm's cosf/atan2f and the two fused multiply-adds.  This script
+trig 2 = libm's cosf/atan2f and the three fused multiply-adds.  This script
 runs the same scenario in two modes and reports, against the tolerance
 max(0.5 s, 1e-4 t):
 

@@ -48,7 +48,7 @@
  * portable arithmetic evaluates with the same float operations, or libm's
  * cosf/atan2f (trig = 1).  trig = 2 follows the reference kernel as nvcc
  * compiles it: libm's cosf/atan2f standing in for CUDA's __cosf/atan2f (which
- * a CPU cannot reproduce bit for bit) and the two multiply-adds of time_from
+ * a CPU cannot reproduce bit for bit) and the three multiply-adds of time_from
  * fused; trig = 3 also takes the cosine and arctangent from tables of the
  * GPU's values (ops_set_tables), so that it follows the reference kernel's
  * arithmetic exactly.  Build with -ffp-contract=off: every other float
@@ -244,12 +244,13 @@ typedef struct {
 static inline int is_boundary(const uint32_t *b, int64_t ix) { return (b[ix >> 5] >> (ix & 31)) & 1u; }
 
 /* time_from, propag.cu:269-294.  The `1.0` literals make the reference
- * evaluate denom and factor in double; that is kept.  With g_trig >= 2 the two
- * sums that nvcc contracts by default (the reference is built without
+ * evaluate denom and factor in double; that is kept.  With g_trig >= 2 the
+ * three sums that nvcc contracts by default (the reference is built without
  * -fmad=false, crates/propag/build.rs:48-69) are fused multiply-adds:
- * dx*dx + dy*dy -> fmaf(dx, dx, dy*dy) and from.time + distance * rcp ->
- * fmaf(distance, rcp, from.time); trig 0 and 1 round every operation on its
- * own. */
+ * 1.0 - e*cos -> fmaf(-e, cos, 1) (nvcc narrows that double subtraction of a
+ * float product to float, exactly, then contracts it), dx*dx + dy*dy ->
+ * fmaf(dx, dx, dy*dy) and from.time + distance * rcp -> fmaf(distance, rcp,
+ * from.time); trig 0 and 1 round every operation on its own. */
 static inline float time_from(const world_t *w, int fx, int fy, float ftime, int tx, int ty,
                               float smax, float azmax, float ecc) {
   const ops_settings_t *s = w->s;
@@ -259,7 +260,7 @@ static inline float time_from(const world_t *w, int fx, int fy, float ftime, int
   else
     azimuth = t_atan2((float)(tx - fx), (float)(ty - fy));
   float angle = fabsf(azimuth - azmax);
-  float denom = (float)(1.0 - (double)(ecc * t_cos(angle)));
+  float denom = g_trig >= 2 ? fmaf(-ecc, t_cos(angle), 1.0f) : (float)(1.0 - (double)(ecc * t_cos(angle)));
   float factor = (float)((1.0 - (double)ecc) * (double)rcp_rd(denom));
   float speed = smax * factor;
   float dx = (float)(fx - tx) * s->dx;

@@ -11,6 +11,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -127,6 +128,18 @@ struct DevBuf {
 };
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Sweeps a job may take before it stops with the sweep-limit status: 2^40
+// (no real scenario comes near), or PROPAG_MAX_SWEEPS from the environment
+// (used by the tests to make the limit run out).
+unsigned long long max_sweeps() {
+  const char *v = std::getenv("PROPAG_MAX_SWEEPS");
+  if (v && *v) {
+    const unsigned long long n = std::strtoull(v, nullptr, 10);
+    if (n > 0) return n;
+  }
+  return 1ull << 40;
+}
 
 bool valid_size(uint32_t w, uint32_t h) { return w >= 1 && h >= 1 && w <= 65534 && h <= 65534; }
 
@@ -400,8 +413,8 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   const size_t upd_max = tn_max + 32 * (team_ctas + 1);
   const size_t ovf_list_bytes = align_up((size_t)csize * ovf_cap * 2, 256);
   const size_t ovf_upd_bytes = align_up((size_t)csize * ovf_cap * sizeof(Update), 256);
-  // two dirty bitmaps and two update arrays (by sweep parity)
-  const size_t slot_bytes = 2 * align_up(words_max * 4, 256) + 2 * align_up(upd_max * sizeof(Update), 256) +
+  // three dirty bitmaps (in rotation) and two update arrays (by sweep parity)
+  const size_t slot_bytes = 3 * align_up(words_max * 4, 256) + 2 * align_up(upd_max * sizeof(TileUpdate), 256) +
                             256 + ovf_list_bytes + ovf_upd_bytes;
   CK(e->slot_scratch.reserve(slot_bytes * n_slots, stream));
   // meta: jobs, slots, stats, queue
@@ -440,9 +453,9 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     sd.dirty = e->slot_scratch.at<uint32_t>(o);
     sd.dirty_words = (uint32_t)(align_up(words_max * 4, 256) / 4);
     sd.pad0 = 0;
-    o += 2 * align_up(words_max * 4, 256);
-    sd.upd = e->slot_scratch.at<Update>(o);
-    o += 2 * align_up(upd_max * sizeof(Update), 256);
+    o += 3 * align_up(words_max * 4, 256);
+    sd.upd = e->slot_scratch.at<TileUpdate>(o);
+    o += 2 * align_up(upd_max * sizeof(TileUpdate), 256);
     sd.ctr = e->slot_scratch.at<uint32_t>(o);
     o += 256;
     sd.ovf_list = e->slot_scratch.at<uint16_t>(o);
@@ -451,7 +464,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
     sd.ovf_cap = (uint32_t)ovf_cap;
     sd.pad = 0;
     // the dirty bitmap and counters must start cleared
-    CK(cudaMemsetAsync(sd.dirty, 0, 2 * align_up(words_max * 4, 256), stream));
+    CK(cudaMemsetAsync(sd.dirty, 0, 3 * align_up(words_max * 4, 256), stream));
     CK(cudaMemsetAsync(sd.ctr, 0, 64, stream));  // counters and barrier arrivals
   }
   JobDev *d_jobs = e->meta.at<JobDev>(0);
@@ -475,7 +488,7 @@ static int engine_run(propag_engine *e, const PropagJob *jobs, uint32_t n_jobs, 
   CK(launch_ignite(d_jobs, n_jobs, stream));
   if (live) CK(cudaEventRecord(e->ev[1], stream));
   CK(launch_engine(d_jobs, n_jobs, d_slots, n_slots, csize, e->threads, smem, d_queue, d_stats,
-                   1ull << 40, d_order, group, group ? e->phantom : 0u, stream));
+                   max_sweeps(), d_order, group, group ? e->phantom : 0u, stream));
   if (live) CK(cudaEventRecord(e->ev[2], stream));
   CK(launch_post(d_jobs, n_jobs, max_cells, e->sms, d_stats, stream));
   if (live) CK(cudaEventRecord(e->ev[3], stream));
@@ -773,8 +786,35 @@ int engine_threads();  // engine.cu: the engine kernel's launch bound
 }
 static_assert(PROPAG_STATIC_MAX_CELLS == kStaticMaxCells, "header and scratch disagree");
 namespace {
+// Device address of the fixed scratch per device ordinal, taken once per
+// device.  It belongs to the device's primary context: after a
+// cudaDeviceReset the process must not call the allocation-free entry
+// points on that device again.
+constexpr int kStaticDevices = 64;
 std::mutex g_static_mu;
-void *g_static_base[64] = {};
+void *g_static_base[kStaticDevices] = {};
+
+void copy_stats(const StatsDev &h, PropagStats &o) {
+  o.rounds = h.rounds;
+  o.launches = h.launches;
+  o.sweeps = h.sweeps;
+  o.evaluations = h.evaluations;
+  o.improvements = h.improvements;
+  o.dda_steps = h.dda_steps;
+  o.gathers = h.gathers;
+  o.refbox_scans = h.refbox_scans;
+  o.burned = h.burned;
+  o.cyc_first = h.cyc_first;
+  o.cyc_eval = h.cyc_eval;
+  o.cyc_commit = h.cyc_commit;
+  o.cyc_stage = h.cyc_stage;
+  o.status = h.status;
+  o.max_walk = h.max_walk;
+  o.t_start_ns = h.t_start_ns;
+  o.t_done_ns = h.t_done_ns;
+  o.scan_cells = h.scan_cells;
+  o.cyc_wait = h.cyc_wait;
+}
 }  // namespace
 
 extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, PropagStats *stats) {
@@ -812,6 +852,7 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   const size_t smem = smem_bytes(tw, th, csize, exact);
   int dev = 0;
   CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticDevices) return fail(PROPAG_ERR_INVALID, "device ordinal out of range");
   char *base = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_static_mu);
@@ -866,35 +907,37 @@ extern "C" int propag_run_device_static(const PropagJob *job, void *stream_ptr, 
   CK(launch_stage_static(d_job, d, d_slot, s, d_stats, d_queue, stream));
   CK(launch_prep(d_job, 1, N, sms, stream));
   CK(launch_ignite(d_job, 1, stream));
-  CK(launch_engine(d_job, 1, d_slot, 1, csize, engine_threads(), smem, d_queue, d_stats, 1ull << 40,
+  CK(launch_engine(d_job, 1, d_slot, 1, csize, engine_threads(), smem, d_queue, d_stats, max_sweeps(),
                    nullptr, 0u, 0u, stream));
   CK(launch_post(d_job, 1, N, sms, d_stats, stream));
   if (stats) {
     StatsDev h;
     CK(cudaMemcpyAsync(&h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    PropagStats &o = *stats;
-    o.rounds = h.rounds;
-    o.launches = h.launches;
-    o.sweeps = h.sweeps;
-    o.evaluations = h.evaluations;
-    o.improvements = h.improvements;
-    o.dda_steps = h.dda_steps;
-    o.gathers = h.gathers;
-    o.refbox_scans = h.refbox_scans;
-    o.burned = h.burned;
-    o.cyc_first = h.cyc_first;
-    o.cyc_eval = h.cyc_eval;
-    o.cyc_commit = h.cyc_commit;
-    o.cyc_stage = h.cyc_stage;
-    o.status = h.status;
-    o.max_walk = h.max_walk;
-    o.t_start_ns = h.t_start_ns;
-    o.t_done_ns = h.t_done_ns;
-    o.scan_cells = h.scan_cells;
-    o.cyc_wait = h.cyc_wait;
+    copy_stats(h, *stats);
     if (h.status) return fail(PROPAG_ERR_TIMEOUT, status_text(h.status));
   }
+  return PROPAG_OK;
+}
+
+extern "C" int propag_static_last_status(void *stream_ptr, PropagStats *stats) {
+  int rc = ensure_device(-1, nullptr);
+  if (rc) return rc;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticDevices) return fail(PROPAG_ERR_INVALID, "device ordinal out of range");
+  char *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    base = static_cast<char *>(g_static_base[dev]);
+  }
+  if (!base) return fail(PROPAG_ERR_INVALID, "no propag_run_device_static call on this device yet");
+  StatsDev h;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  CK(cudaMemcpyAsync(&h, base + kStaticStatsOff, sizeof(h), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (stats) copy_stats(h, *stats);
+  if (h.status) return fail(PROPAG_ERR_TIMEOUT, status_text(h.status));
   return PROPAG_OK;
 }
 

@@ -414,16 +414,29 @@ __device__ __forceinline__ void sync_cluster() {
 // ---- team synchronisation ----
 // The CTAs that work on one job meet at every phase boundary: at the hardware
 // cluster barrier, or in group mode (G CTAs of a cooperative launch without
-// clusters, tiles in global memory) at an arrival counter in global memory.
-// A group wait is bounded: when the other CTAs have not all arrived after
-// kGroupWaitNs, or once any CTA of the launch has given up, it sets the
-// launch's error flag and returns false, and the caller abandons the launch.
+// clusters, tiles in global memory) at an arrival word in global memory.
+// Group mode alternates between two 64-bit arrival words (barrier k uses
+// word k & 1): a CTA arrives with one release reduction adding 1 to the low
+// half and, when it improved a cell in the sweep that ends there, 1 to the
+// high half; the barrier is complete when the low half reaches the team's
+// running target, and the high half's growth since the word's last use is
+// the number of CTAs that improved.  The count is exact: a CTA can add to
+// word k & 1 again only at barrier k + 2, which no CTA reaches before every
+// CTA has arrived at barrier k + 1, i.e. has finished reading barrier k.
+// (The low half carries into the high half after 2^32 arrivals on one word,
+// billions of sweeps.)  A group wait is bounded: when the other CTAs have
+// not all arrived after kGroupWaitNs, or once any CTA of the launch has
+// given up, it sets the launch's error flag and returns false, and the
+// caller abandons the launch.
 constexpr unsigned long long kGroupWaitNs = 2000000000ull;  // 2 s; a phase takes < 50 ms
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
+}
+__device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
   uint32_t v;
@@ -432,42 +445,76 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
 }
 
 struct Team {
-  unsigned long long *bar;  // group mode: arrivals at the group's barriers; null = cluster
+  unsigned long long *bar;  // group mode: the two arrival words; null = cluster
   uint32_t *err;            // group mode: the launch's error flag
-  int *ok;                  // shared: this CTA's outcome of the last wait
+  int *ok;                  // shared: [0] this CTA's outcome of the last wait, [1] improving CTAs
   uint32_t G;               // CTAs in the group
-  unsigned long long target = 0;
+  uint32_t phase = 0;       // thread 0: barriers passed
+  uint32_t target[2] = {0u, 0u};  // thread 0: arrivals expected on each word (low half, modular)
+  uint32_t seen[2] = {0u, 0u};    // thread 0: the high half of each word at its last use
   unsigned long long waited = 0;  // thread 0: cycles from arrival to release
-  // global_fence = false: cluster mode orders shared-memory accesses only
-  __device__ bool sync(bool global_fence = true) {
+  // Cluster mode's count of improving CTAs: three counters in global memory
+  // used in rotation by the barriers that count (barrier k: counter k % 3).
+  // The cluster's leader clears counter (k + 2) % 3 after barrier k: it was
+  // last read right after barrier k - 1, and no CTA adds to it before it has
+  // passed barrier k + 1, which the leader reaches after the clear.
+  uint32_t *cnt3 = nullptr;
+  bool cnt_leader = false;
+  uint32_t dsweep = 0;  // every thread: sweeps of global-memory tiles (dirty bitmap rotation)
+  uint32_t cnt_phase = 0;  // thread 0: counting barriers passed, mod 3
+  // global_fence = false: cluster mode orders shared-memory accesses only.
+  // improved: this CTA improved a cell in the phase that ends here;
+  // *improving receives the number of the team's CTAs that did.
+  __device__ bool sync(bool global_fence = true, bool improved = false, uint32_t *improving = nullptr) {
     const long long t0 = threadIdx.x == 0 ? clock64() : 0;
     if (!bar) {
-      if (global_fence) __threadfence();
+      if (improving && threadIdx.x == 0 && improved) atomicAdd(cnt3 + cnt_phase, 1u);
+      if (global_fence || improving) __threadfence();
       cg::this_cluster().sync();
-      if (threadIdx.x == 0) waited += (unsigned long long)(clock64() - t0);
+      if (threadIdx.x == 0) {
+        if (improving) {
+          ok[1] = (int)__ldcg(cnt3 + cnt_phase);
+          if (cnt_leader) cnt3[(cnt_phase + 2) % 3] = 0u;
+          cnt_phase = (cnt_phase + 1) % 3;
+        }
+        waited += (unsigned long long)(clock64() - t0);
+      }
+      if (improving) {
+        __syncthreads();
+        *improving = (uint32_t)ok[1];
+      }
       return true;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      target += G;  // every CTA of the group passes the same barriers
-      __threadfence();
-      atomicAdd(bar, 1ull);
+      const uint32_t w = phase & 1u;
+      ++phase;
+      target[w] += G;  // every CTA of the group passes the same barriers
+      unsigned long long *word = bar + w;
+      // the release orders this CTA's writes (made visible to thread 0 by the
+      // CTA barrier above) before the arrival
+      red_release_add_u64(word, 1ull | ((unsigned long long)(improved ? 1u : 0u) << 32));
       bool good = true;
       const unsigned long long start_ns = globaltimer_ns();
-      while (ld_acquire_u64(bar) < target) {
+      unsigned long long v = ld_acquire_u64(word);
+      while ((int32_t)((uint32_t)v - target[w]) < 0) {
         if (ld_relaxed_u32(err) != 0u || globaltimer_ns() - start_ns > kGroupWaitNs) {
           good = false;
           break;
         }
         __nanosleep(32);
+        v = ld_acquire_u64(word);
       }
       if (!good) atomicOr(err, 1u);
-      __threadfence();
-      *ok = good ? 1 : 0;
+      const uint32_t hi = (uint32_t)(v >> 32);
+      ok[0] = good ? 1 : 0;
+      ok[1] = (int)(hi - seen[w]);
+      seen[w] = hi;
       waited += (unsigned long long)(clock64() - t0);
     }
     __syncthreads();
-    return *ok != 0;
+    if (improving) *improving = (uint32_t)ok[1];
+    return ok[0] != 0;
   }
 };
 
@@ -553,11 +600,11 @@ __device__ __forceinline__ void mark3x3_pending(uint32_t *dirty, uint32_t *pendi
 }
 
 // Takes (reads and clears) the pending bits of tile cells k0 .. k0 + n - 1
-// (n <= 32, tile-linear order) from the grid-wide bitmap; bit i of the
-// result is cell k0 + i.  The cells of one tile row are consecutive grid
+// (n <= 32, tile-linear order) selected by mask (bit i: cell k0 + i) from
+// the grid-wide bitmap; bit i of the result is cell k0 + i.  The cells of one tile row are consecutive grid
 // cells, so each row segment is a funnel shift of two words.
 __device__ __forceinline__ uint32_t take_pending(uint32_t *pending, const JobDev &j, int x0, int y0,
-                                                 int TW, uint32_t k0, uint32_t n) {
+                                                 int TW, uint32_t k0, uint32_t n, uint32_t mask) {
   uint32_t out = 0, done = 0;
   while (done < n) {
     const uint32_t k = k0 + done;
@@ -570,7 +617,7 @@ __device__ __forceinline__ uint32_t take_pending(uint32_t *pending, const JobDev
     const uint64_t w2 =
         (uint64_t)__ldcg(pending + wi) | (two ? (uint64_t)__ldcg(pending + wi + 1) << 32 : 0ull);
     const uint32_t m = seg >= 32 ? 0xFFFFFFFFu : (1u << seg) - 1u;
-    const uint32_t bits = (uint32_t)(w2 >> sh) & m;
+    const uint32_t bits = (uint32_t)(w2 >> sh) & m & (mask >> done);
     if (bits) {
       const uint64_t cm = (uint64_t)bits << sh;
       if ((uint32_t)cm) atomicAnd(pending + wi, ~(uint32_t)cm);
@@ -599,19 +646,74 @@ struct SweepCtx {
   }
 };
 
+// Ownership of a global-memory tile's cells: the tile-linear cells are cut
+// into groups of kOwnGroup consecutive cells, and group g belongs to CTA
+// g mod R of the team, so that the cells of a front spread over the CTAs
+// while a CTA's cells still come in short runs (its neighbour reads share
+// L1 lines).  Tile word w (cells 32 w .. 32 w + 31) holds kGroupsPerWord
+// groups; CTA `rank` owns those at offsets first, first + R, ... of the word.
+// Groups of 4 cells measured fastest on the 4096^2 scenario with 148 CTAs
+// (769 ms; 1 cell: 787 ms; whole 32-cell words dealt round-robin, with
+// the scan of every word: slower still).
+constexpr uint32_t kOwnGroup = 4;  // a power of two, at most 32
+constexpr uint32_t kGroupsPerWord = 32u / kOwnGroup;
+__device__ __forceinline__ uint32_t owned_first(uint32_t w, uint32_t rank, uint32_t R) {
+  return (rank + R - (w * kGroupsPerWord) % R) % R;  // offset of the first owned group of word w
+}
+__device__ __forceinline__ uint32_t owned_mask(uint32_t first, uint32_t R) {
+  constexpr uint32_t g = kOwnGroup == 32u ? 0xFFFFFFFFu : (1u << kOwnGroup) - 1u;
+  uint32_t m = 0;
+  for (uint32_t i = first; i < kGroupsPerWord; i += R) m |= g << (i * kOwnGroup);
+  return m;
+}
+// Owned cells of one word at most: kOwnGroup per owned group.
+__host__ __device__ inline uint32_t owned_per_word(uint32_t R) {
+  return kOwnGroup * ((kGroupsPerWord + R - 1) / R);
+}
+constexpr int kScanBatch = 8;  // dirty words a thread loads at once
+
+// A global-memory tile's update entries of one sweep: this CTA's first
+// kTileUpdSmem in shared memory, the rest in its global update region.
+__device__ __forceinline__ TileUpdate get_update(const TileUpdate *sm_upd, const TileUpdate *g_upd,
+                                                 uint32_t u) {
+  if (u < (uint32_t)kTileUpdSmem) return sm_upd[u];
+  const uint4 *q = reinterpret_cast<const uint4 *>(g_upd + u);
+  const uint4 a = __ldcg(q), b = __ldcg(q + 1);
+  return TileUpdate{a.x, __uint_as_float(a.y), a.z, a.w, b.x, b.y, 0u, 0u};
+}
+
 // One tile launch with the state in global memory, by a team of R CTAs
 // (this one is `rank`).  `list` is shared memory for blockDim.x * 32 u16
-// entries, `cta_ctr` two shared counters.  Returns whether any sweep
-// improved a cell.
+// entries, `sm_upd` for two sweeps' kTileUpdSmem update entries, `cta_ctr`
+// two shared counters.  Returns whether any sweep improved a cell.
+//
+// An update entry carries what the commit needs besides the new time and
+// reference: whether the cell burns (its neighbours read it) and its
+// referrer box, both read while the cell is evaluated, so that the commit
+// makes no dependent global reads.  The box read then (before or during
+// other CTAs' commits of the sweep) holds every referrer adopted in earlier
+// sweeps (their growth happened before the last barrier); referrers that
+// adopt the cell in this sweep improved, and mark their neighbourhoods
+// themselves.  Concurrent growth can only widen the box (a box created in
+// this sweep may show the empty marker in a corner: corners are clamped to
+// the grid), which costs scan work, never a mark: a scan hits the cells that
+// referenced the cell when the sweep started.  With a pending bitmap the
+// scans read referrers outside the launching tile too, from X[p]: a launch
+// writes only its tile's cells, and both copies agree everywhere when a
+// launch ends, so outside the tile X[0] and X[1] hold the same state.
 __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &s, const TileDesc &td,
-                            ScanBox *scan_boxes, uint16_t *list, uint32_t *cta_ctr, uint32_t rank,
-                            uint32_t R, SweepCtx &cx, Team &team) {
+                            ScanBox *scan_boxes, uint32_t *list, TileUpdate *sm_upd, uint32_t *cta_ctr,
+                            uint32_t rank, uint32_t R, SweepCtx &cx, Team &team) {
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int x0 = td.x0, y0 = td.y0, TW = td.TW, TH = td.TH;
   const uint32_t TN = (uint32_t)TW * (uint32_t)TH;
   const uint32_t nwords = (TN + 31) / 32;
-  const uint32_t mine = nwords > rank ? (nwords - rank + R - 1) / R : 0u;  // words of this CTA
+  // a chunk of words yields at most the list's capacity of owned cells: the
+  // whole tile when this CTA's share fits, else a bounded run of words
   const uint32_t cap = global_tile_upd_cap(TN, R);
+  const uint32_t chunk_words = cap <= global_tile_list_cap(blockDim.x)
+                                   ? nwords
+                                   : global_tile_list_cap(blockDim.x) / owned_per_word(R);
   float *const tm[2] = {j.time, j.time1};
   uint32_t *const rf[2] = {j.refs, j.refs1};
   // the launch's counters in registers (the context may live in local memory)
@@ -619,43 +721,72 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
   bool first = true, worked = false;
   uint32_t prev_upd = 0;  // this CTA's improvements of the previous sweep
   int p = 0;              // sweep parity: read X[p], write X[p ^ 1]
-  // The team's improvement count of a sweep rotates over three counters
-  // (s.ctr[5..7]): the one of sweep s - 1 is cleared after sweep s's barrier,
-  // when every CTA has read it and none can add to it before the next barrier.
-  int q = 0;
   for (;;) {
     ++cx.sweeps;  // every thread counts, so the abort below is uniform
     const float *const rt = tm[p];
     const uint32_t *const rr = rf[p];
     float *const wt = tm[p ^ 1];
     uint32_t *const wr = rf[p ^ 1];
-    uint32_t *const dirty = s.dirty + (size_t)p * s.dirty_words;
-    uint32_t *const dirty_next = s.dirty + (size_t)(p ^ 1) * s.dirty_words;
-    Update *const upd = s.upd + ((size_t)p * R + rank) * cap;
-    const Update *const upd_prev = s.upd + ((size_t)(p ^ 1) * R + rank) * cap;
+    // dirty bitmaps in rotation by the team's sweep count d: read D[d % 3],
+    // mark D[(d + 1) % 3], clear D[(d + 2) % 3] (read in sweep d - 1)
+    const uint32_t dsw = team.dsweep++;
+    uint32_t *const dirty = s.dirty + (size_t)(dsw % 3) * s.dirty_words;
+    uint32_t *const dirty_next = s.dirty + (size_t)((dsw + 1) % 3) * s.dirty_words;
+    uint32_t *const dirty_old = s.dirty + (size_t)((dsw + 2) % 3) * s.dirty_words;
+    TileUpdate *const upd = s.upd + ((size_t)p * R + rank) * cap;
+    const TileUpdate *const upd_prev = s.upd + ((size_t)(p ^ 1) * R + rank) * cap;
+    TileUpdate *const supd = sm_upd + p * kTileUpdSmem;
+    const TileUpdate *const supd_prev = sm_upd + (p ^ 1) * kTileUpdSmem;
     // ---- 1, 2: compact and evaluate (nothing is written to X[p]) ----
+    // the bitmap read two sweeps ago is cleared now (its marks come in the
+    // next sweep): the words w = rank mod R of the slot's bitmap
+    for (uint32_t w = rank + threadIdx.x * R; w < s.dirty_words; w += blockDim.x * R) dirty_old[w] = 0u;
     if (threadIdx.x == 0) cta_ctr[1] = 0;
-    for (uint32_t c0 = 0; c0 < mine; c0 += blockDim.x) {
+    for (uint32_t c0 = 0; c0 < nwords; c0 += chunk_words) {
       __syncthreads();  // the previous chunk's list is consumed
       if (threadIdx.x == 0) cta_ctr[0] = 0;
       __syncthreads();
-      const uint32_t t = c0 + threadIdx.x;  // this CTA's t-th word
-      uint32_t bits = 0;
-      if (t < mine) {
-        const uint32_t w = rank + t * R;
-        if (first) {
-          const uint32_t nb = (w == nwords - 1 && (TN & 31)) ? (TN & 31) : 32u;
-          // the whole tile, or with a pending bitmap the cells whose inputs
-          // changed since their last evaluation
-          bits = j.pending ? take_pending(j.pending, j, x0, y0, TW, w * 32, nb)
-                           : (nb == 32 ? 0xFFFFFFFFu : (1u << nb) - 1u);
-        } else {
-          bits = __ldcg(dirty + w);
-          if (bits) dirty[w] = 0u;
+      const uint32_t c1 = min(nwords, c0 + chunk_words);
+      // this thread's words w = c0 + threadIdx.x + i blockDim.x, in batches of
+      // kScanBatch whose loads all go out before any is used; the offset of
+      // the first owned group of word w steps by a constant from one word to
+      // the next of the thread
+      uint32_t fo = owned_first(c0 + threadIdx.x, rank, R);
+      const uint32_t fstep = (R - (kGroupsPerWord * blockDim.x) % R) % R;
+      for (uint32_t wb = c0 + threadIdx.x; wb < c1; wb += kScanBatch * blockDim.x) {
+        uint32_t v[kScanBatch];
+#pragma unroll
+        for (int i = 0; i < kScanBatch; ++i) {
+          const uint32_t w = wb + (uint32_t)i * blockDim.x;
+          v[i] = 0u;
+          if (w < c1) {
+            if (!first) {
+              v[i] = __ldcg(dirty + w);
+            } else if (!j.pending) {  // the whole tile
+              const uint32_t nb = (w == nwords - 1 && (TN & 31)) ? (TN & 31) : 32u;
+              v[i] = nb == 32 ? 0xFFFFFFFFu : (1u << nb) - 1u;
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < kScanBatch; ++i) {
+          const uint32_t w = wb + (uint32_t)i * blockDim.x;
+          const uint32_t own = owned_mask(fo, R);
+          fo += fstep;
+          if (fo >= R) fo -= R;
+          if (w >= c1) continue;
+          uint32_t bits = v[i] & own;
+          if (first && j.pending) {
+            // the cells whose inputs changed since their last evaluation
+            const uint32_t nb = (w == nwords - 1 && (TN & 31)) ? (TN & 31) : 32u;
+            bits = take_pending(j.pending, j, x0, y0, TW, w * 32, nb, own);
+          }
+          if (bits) {
+            uint32_t at = atomicAdd(cta_ctr + 0, (uint32_t)__popc(bits));
+            for (; bits; bits &= bits - 1) list[at++] = w * 32 + (uint32_t)(__ffs(bits) - 1);
+          }
         }
       }
-      uint32_t at = warp_append(cta_ctr + 0, __popc(bits), lane);
-      for (; bits; bits &= bits - 1) list[at++] = (uint16_t)(threadIdx.x * 32 + __ffs(bits) - 1);
       __syncthreads();
       const uint32_t nlist = cta_ctr[0];
       if (threadIdx.x == 0) cnt.evals += nlist;
@@ -666,28 +797,58 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
         uint32_t k = 0;
         int x = 0, y = 0;
         Best own{FLT_MAX, kNoRef};
+        uint32_t bx0 = kEmptyBox, by0 = 0, bx1 = 0, by1 = 0;
+        float own_speed = 0.0f;
         if (valid) {
-          const uint32_t e = list[ci];
-          k = (rank + (c0 + (e >> 5)) * R) * 32 + (e & 31);
+          k = list[ci];
           x = x0 + (int)(k % (uint32_t)TW);
           y = y0 + (int)(k / (uint32_t)TW);
           const int64_t c = x + (int64_t)y * j.W;
           own = Best{__ldcg(rt + c), __ldcg(rr + c)};
+          if ((lane & 7) == 0) {  // what the commit needs if the cell improves
+            own_speed = __ldg(j.speed + c);
+            bx0 = __ldcg(j.box_x0 + c);
+            by0 = __ldcg(j.box_y0 + c);
+            bx1 = __ldcg(j.box_x1 + c);
+            by1 = __ldcg(j.box_y1 + c);
+          }
         }
         const Best b = evaluate_coop(j, dc, GlobalAcc{j, rt, rr}, x, y, own, valid, lane, cnt);
         const bool improved = valid && (lane & 7) == 0 && b.time < own.time;
         const uint32_t ai = warp_append(cta_ctr + 1, improved ? 1u : 0u, lane);
-        if (improved) upd[ai] = Update{k, b.time, b.ref, 0u};
+        if (improved) {
+          Box box{1, 1, 0, 0};
+          if (bx0 != kEmptyBox) {
+            if (j.pending)  // the whole box: referrers anywhere mark pending cells
+              box = Box{max((int)bx0, 0), max((int)by0, 0), min((int)bx1, j.W - 1), min((int)by1, j.H - 1)};
+            else
+              box = clip_box((int)bx0, (int)by0, (int)bx1, (int)by1, x0, y0, TW, TH, j.W, j.H);
+          }
+          // corners in 16 bits (grids up to 65534 cells a side); an empty box
+          // as x0 = 0xFFFF > x1
+          const bool empty = box.x0 > box.x1 || box.y0 > box.y1;
+          const uint32_t b01 = empty ? 0xFFFFu : (uint32_t)box.x0 | ((uint32_t)box.y0 << 16);
+          const uint32_t b23 = empty ? 0u : (uint32_t)box.x1 | ((uint32_t)box.y1 << 16);
+          // only a burning cell is read by its neighbours
+          const uint32_t burn = b.time < j.max_time && own_speed != 0.0f ? 1u : 0u;
+          if (ai < (uint32_t)kTileUpdSmem) {
+            supd[ai] = TileUpdate{k, b.time, b.ref, burn, b01, b23, 0u, 0u};
+          } else {
+            uint4 *q = reinterpret_cast<uint4 *>(upd + ai);
+            q[0] = make_uint4(k, __float_as_uint(b.time), b.ref, burn);
+            q[1] = make_uint4(b01, b23, 0u, 0u);
+          }
+        }
       }
     }
     __syncthreads();
     const uint32_t my_upd = cta_ctr[1];
     // ---- 3a: the previous sweep's improvements into X[p ^ 1] ----
     for (uint32_t u = threadIdx.x; u < prev_upd; u += blockDim.x) {
-      const uint4 raw = __ldcg(reinterpret_cast<const uint4 *>(upd_prev) + u);  // Update{k, time, ref}
-      const int64_t c = (x0 + (int)(raw.x % (uint32_t)TW)) + (int64_t)(y0 + (int)(raw.x / (uint32_t)TW)) * j.W;
-      wt[c] = __uint_as_float(raw.y);
-      wr[c] = raw.z;
+      const TileUpdate e = get_update(supd_prev, upd_prev, u);
+      const int64_t c = (x0 + (int)(e.k % (uint32_t)TW)) + (int64_t)(y0 + (int)(e.k / (uint32_t)TW)) * j.W;
+      wt[c] = e.time;
+      wr[c] = e.ref;
     }
     __syncthreads();  // this sweep's improvements of the same cells land after
     // ---- 3b: commit (update_point / commit_point), mark, referrer scans.
@@ -697,41 +858,25 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
     for (uint32_t base = warp * per; base < my_upd; base += nwarps * per) {
       const uint32_t u = base + lane;
       const bool valid = lane < per && u < my_upd;
-      int lx = 0, ly = 0;
       uint32_t want = 0;
       Box box{1, 1, 0, 0};
       if (valid) {
-        const uint4 raw = __ldcg(reinterpret_cast<const uint4 *>(upd) + u);  // Update{k, time, ref}
-        const float ut = __uint_as_float(raw.y);
-        lx = (int)(raw.x % (uint32_t)TW);
-        ly = (int)(raw.x / (uint32_t)TW);
+        const TileUpdate e = get_update(supd, upd, u);
+        const int lx = (int)(e.k % (uint32_t)TW), ly = (int)(e.k / (uint32_t)TW);
         const int x = x0 + lx, y = y0 + ly;
         const int64_t c = x + (int64_t)y * j.W;
-        wt[c] = ut;
-        wr[c] = raw.z;
-        box_expand_global(j, raw.z, x, y);
-        // only a burning cell is read by its neighbours
-        if (ut < j.max_time && __ldg(j.speed + c) != 0.0f) {
+        wt[c] = e.time;
+        wr[c] = e.ref;
+        box_expand_global(j, e.ref, x, y);
+        if (e.burn) {
           if (j.pending)
             mark3x3_pending(dirty_next, j.pending, j, x0, y0, lx, ly, TW, TH);
           else
             mark3x3_bits(dirty_next, lx, ly, TW, TH);
         }
         want = pack_ref(x, y);
-        const uint32_t bx0 = __ldcg(j.box_x0 + c);
-        if (bx0 != kEmptyBox) {
-          if (j.pending)  // the whole box: referrers anywhere mark pending cells
-            // clamped to the grid: a box that another lane creates in this
-            // sweep can show the empty marker (0xFFFFFFFF, -1 as int) in its
-            // other corner; such a box had no referrers before this sweep,
-            // and this sweep's referrers mark their neighbourhoods themselves
-            box = Box{max((int)bx0, 0), max((int)__ldcg(j.box_y0 + c), 0),
-                      min((int)__ldcg(j.box_x1 + c), j.W - 1),
-                      min((int)__ldcg(j.box_y1 + c), j.H - 1)};
-          else
-            box = clip_box((int)bx0, (int)__ldcg(j.box_y0 + c), (int)__ldcg(j.box_x1 + c),
-                           (int)__ldcg(j.box_y1 + c), x0, y0, TW, TH, j.W, j.H);
-        }
+        if ((e.b01 & 0xFFFFu) != 0xFFFFu)
+          box = Box{(int)(e.b01 & 0xFFFFu), (int)(e.b01 >> 16), (int)(e.b23 & 0xFFFFu), (int)(e.b23 >> 16)};
       }
       warp_scan_boxes(
           scan_boxes + (threadIdx.x & ~31u), box, want, j, lane, cnt,
@@ -748,23 +893,18 @@ __device__ bool tile_global(const JobDev &j, const DirConst &dc, const SlotDev &
               mark3x3_bits(dirty_next, xx - x0, yy - y0, TW, TH);
           });
     }
-    // ---- 4: count, meet ----
-    if (threadIdx.x == 0 && my_upd) atomicAdd(s.ctr + 5 + q, my_upd);
-    if (!team.sync()) {
+    // ---- 4: meet; the barrier reports how many CTAs improved a cell ----
+    uint32_t improving = 0;
+    if (!team.sync(true, my_upd > 0, &improving)) {
       cx.failed = cx.abort = true;
       break;
     }
     cx.tick(first ? 0 : 1);
-    const uint32_t nupd = __ldcg(s.ctr + 5 + q);
-    // the previous sweep's count (zero when this launch ends here, so that
-    // the next tile launch finds all three at zero)
-    if (cx.leader) s.ctr[5 + (q == 0 ? 2 : q - 1)] = 0;
-    if (nupd == 0) break;  // X[p ^ 1] got the last improvements: both copies agree
+    if (threadIdx.x == 0) cx.improvements += my_upd;  // summed over the team at the job's end
+    if (improving == 0) break;  // X[p ^ 1] got the last improvements: both copies agree
     worked = true;
-    if (cx.leader) cx.improvements += nupd;
     prev_upd = my_upd;
     p ^= 1;
-    q = q == 2 ? 0 : q + 1;
     first = false;
     if (cx.sweeps > cx.max_sweeps) {
       cx.abort = true;
@@ -1239,10 +1379,12 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
   __shared__ DirConst dc;
   __shared__ JobDev js;
   __shared__ ScanBox scan_boxes[kEngineThreads];
-  __shared__ int team_ok;
+  __shared__ int team_ok[2];
   __shared__ uint32_t cta_ctr[2];  // global-memory tiles: work list and update counts
   Team team{grouped ? reinterpret_cast<unsigned long long *>(s.ctr + 8) : nullptr, queue + 1,
-            &team_ok, csize};
+            team_ok, csize};
+  team.cnt3 = s.ctr + 5;  // cluster mode: slot counters 5..7
+  team.cnt_leader = rank == 0;
   uint32_t taken = 0xFFFFFFFFu;  // tid 0: the queue position it took last
 
   for (;;) {
@@ -1250,7 +1392,6 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
       taken = atomicAdd(queue, 1u);
       s.ctr[4] = taken;
       s.ctr[0] = s.ctr[1] = s.ctr[2] = s.ctr[3] = 0;
-      s.ctr[5] = s.ctr[6] = s.ctr[7] = 0;
     }
     if (!team.sync()) break;
     // teams take the jobs in queue order; `order` (when given) maps queue
@@ -1286,8 +1427,10 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
                        : j.smem_tile == kSmemTileCoarse
                            ? tile_smem<BoxCoarse>(j, dc, dyn_smem, s, td, scan_boxes, cx, team)
                            : tile_global(j, dc, s, td, scan_boxes,
-                                         reinterpret_cast<uint16_t *>(dyn_smem), cta_ctr, rank,
-                                         csize, cx, team);
+                                         reinterpret_cast<uint32_t *>(dyn_smem),
+                                         reinterpret_cast<TileUpdate *>(
+                                             dyn_smem + global_tile_list_bytes(blockDim.x)),
+                                         cta_ctr, rank, csize, cx, team);
         round_worked |= w;
       }
       if (!round_worked || cx.abort) break;
@@ -1311,11 +1454,13 @@ __global__ void __launch_bounds__(kEngineThreads, 1) engine_kernel(const JobDev 
       if (evals) atomicAdd(&st->evaluations, evals);
       if (cnt.walk_max) atomicMax(&st->max_walk, cnt.walk_max);
     }
+    // every CTA's own improvements (global-memory tiles), or the cluster's
+    // total counted by its leader (shared-memory tiles)
+    if (threadIdx.x == 0 && cx.improvements) atomicAdd(&st->improvements, cx.improvements);
     if (cx.leader) {
       st->rounds = rounds;
       st->launches = launches;
       st->sweeps = cx.sweeps;
-      st->improvements = cx.improvements;
       st->cyc_first = cx.cyc[0];
       st->cyc_eval = cx.cyc[1];
       st->cyc_commit = cx.cyc[2];

@@ -51,20 +51,40 @@ struct Update {
 };
 static_assert(sizeof(Update) == 16, "an update is read back as one 16-byte load");
 
+// An improvement of a global-memory tile's sweep, with what its commit needs:
+// burn = the cell burns (time < max_time, own fire not null); its referrer
+// box as read during the evaluation, corners (x0, y0), (x1, y1) in 16 bits
+// each (b01 = x0 | y0 << 16, b23 = x1 | y1 << 16; x0 = 0xFFFF: empty).
+struct TileUpdate {
+  uint32_t k;  // cell index inside the tile
+  float time;
+  uint32_t ref;
+  uint32_t burn;
+  uint32_t b01, b23;
+  uint32_t pad[2];
+};
+static_assert(sizeof(TileUpdate) == 32, "two 16-byte halves");
+// Update entries a CTA keeps in shared memory per sweep parity (the rest go
+// to its global update region).
+constexpr int kTileUpdSmem = 1024;
+
 // Global-memory scratch of one team slot.  dirty/upd serve tile launches
-// whose state stays in global memory: the tile's dirty bitmaps and the
+// whose state stays in global memory: the tile's dirty bitmaps (read by
+// every CTA of the team: a tile's cells are dealt to the CTAs in groups) and the
 // update arrays (one per sweep parity), CTA r of an R-CTA team using entries
-// from (parity * R + r) * cap on (cap = global_tile_upd_cap); ovf_list/ovf_upd take the work-list and update-list
-// entries of shared-memory tiles beyond their shared-memory capacity
-// (ovf_cap entries per CTA of the cluster, CTA r at offset r * ovf_cap).
+// from (parity * R + r) * cap on (cap = global_tile_upd_cap; the first
+// kTileUpdSmem of them stay in shared memory); ovf_list/ovf_upd take the
+// work-list and update-list entries of shared-memory tiles beyond their
+// shared-memory capacity (ovf_cap entries per CTA of the cluster, CTA r at
+// offset r * ovf_cap).
 struct SlotDev {
-  uint32_t *dirty;        // two bitmaps of dirty_words words (by sweep parity)
+  uint32_t *dirty;        // three bitmaps of dirty_words words (in rotation by sweep)
   uint32_t dirty_words;
   uint32_t pad0;
-  Update *upd;
-  // [0..3] shared-memory tiles' counters, [4] job, [5..7] global-memory
-  // tiles' improvement counts (rotating by sweep), [8..9] group-mode barrier
-  // arrivals (64-bit)
+  TileUpdate *upd;
+  // [0..3] shared-memory tiles' counters, [4] job, [5..7] cluster mode's
+  // improving-CTA counts of global-memory tiles (rotating by barrier),
+  // [8..11] group mode's two 64-bit barrier arrival words
   uint32_t *ctr;
   uint16_t *ovf_list;
   Update *ovf_upd;
@@ -73,16 +93,23 @@ struct SlotDev {
 };
 
 // Update-array entries a CTA of an R-CTA team may need in one sweep of a
-// global-memory tile of TN cells (the cells of its bitmap words); the team
-// needs R times that, at most TN + 32 R.
+// global-memory tile of TN cells (the cells it owns: groups of up to 32
+// consecutive cells dealt round-robin); the team needs R times that, at most
+// TN + 32 R.
 __host__ __device__ inline uint32_t global_tile_upd_cap(uint32_t TN, uint32_t R) {
-  const uint32_t nwords = (TN + 31) / 32;
-  return (nwords + R - 1) / R * 32;
+  return ((TN + 31) / 32 + R - 1) / R * 32;
 }
 
-// Shared memory a CTA needs for a global-memory tile launch: the u16 work
-// list of one chunk (32 cells of each of blockDim.x words).
-__host__ __device__ inline size_t global_tile_smem(int threads) { return (size_t)threads * 32 * 2; }
+// Shared memory a CTA needs for a global-memory tile launch: the work list
+// of one chunk (tile cell indices, 32 per thread), then two sweeps' update
+// entries.
+__host__ __device__ inline uint32_t global_tile_list_cap(int threads) { return (uint32_t)threads * 32u; }
+__host__ __device__ inline size_t global_tile_list_bytes(int threads) {
+  return (size_t)global_tile_list_cap(threads) * 4;
+}
+__host__ __device__ inline size_t global_tile_smem(int threads) {
+  return global_tile_list_bytes(threads) + 2 * kTileUpdSmem * sizeof(TileUpdate);
+}
 
 // Per-job statistics accumulated on the device (PropagStats order).
 struct StatsDev {

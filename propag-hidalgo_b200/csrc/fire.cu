@@ -13,10 +13,16 @@
 // Layout and mapping: one cell per thread, grid-stride, so that every load
 // and store of a warp is one coalesced run (4 bytes per lane, 1 for the fuel
 // codes); the grid holds as many CTAs as are resident at once (one wave),
-// and 32-bit indices serve every grid below 2^32 cells.  The fuel table sits in
-// shared memory (20 models x 64 floats), indexed per cell.  Double-float
+// and 32-bit indices serve every grid below 2^32 cells.  Four cells per thread
+// with 128-bit loads measured slower (0.298 against 0.277 ms at 4096^2): the
+// pass is bound by instruction issue, and four inlined copies of the cell
+// code overflow the instruction cache.  The fuel table sits in shared memory
+// with a row stride of 65 words (20 models), so that the lanes of a warp that
+// read the same field of different models hit different banks.  Double-float
 // moisture sums measured faster here than FP64 ones (0.33-0.35 ms against
-// 0.35-0.36 ms at 4096^2).
+// 0.35-0.36 ms at 4096^2).  Compiled without automatic multiply-add
+// contraction, so that the 3-field and 10-field instantiations round alike
+// (contraction measured no faster).
 //
 // FP32 formulation.  The arithmetic is the reference's, rearranged where the
 // float evaluation of the literal formula loses accuracy against double:
@@ -167,8 +173,12 @@ __device__ __forceinline__ void burn_cell(const FuelConst &F, const float m[5], 
     // speed0 > 0 is kept out: (x, y) below are those vectors / speed0, the
     // direction and quadrant are unchanged and phi_ew2 = |(x, y)|.
     const float split = upslope <= waz ? waz - upslope : ((kTwoPiHi - upslope) + waz) + kTwoPiLo;
+    // the same angle in [-pi, pi], where the fast sine and cosine are
+    // accurate to 2^-21.4 absolute (the vector components are then good to
+    // ~4e-7 of phi_wind, inside the fields' 1e-5 budget)
+    const float red = split > kPiHi ? (split - kTwoPiHi) - kTwoPiLo : split;
     float sn, cs;
-    sincosf(split, &sn, &cs);
+    __sincosf(red, &sn, &cs);
     const float x = fmaf(phi_wind, cs, phi_slope);
     const float y = phi_wind * sn;
     pew = sqrtf(fmaf(x, x, y * y));  // phi values far below 1e18: no overflow to guard
@@ -224,59 +234,76 @@ __device__ __forceinline__ void store_cell(const Outputs &out, Index i, const Fi
     if ((kFull || (k >= 4 && k <= 6)) && out.f[k]) out.f[k][i] = v[k];
 }
 
+// Shared-memory copy of the fuel table, rows kCatStride words apart (odd:
+// the same field of different models lies in different banks).
+constexpr int kCatStride = 65;
+static_assert(sizeof(FuelConst) / 4 <= kCatStride, "a FuelConst fits a table row");
+
+__device__ __forceinline__ void load_catalog(float *cat) {
+  const float *src = reinterpret_cast<const float *>(c_catalog);
+  constexpr int kWords = (int)(sizeof(FuelConst) / 4);
+  for (int t = threadIdx.x; t < kMaxFuels * kWords; t += blockDim.x)
+    cat[(t / kWords) * kCatStride + t % kWords] = src[t];
+  __syncthreads();
+}
+
+__device__ __forceinline__ const FuelConst &fuel_row(const float *cat, uint32_t code) {
+  return *reinterpret_cast<const FuelConst *>(cat + code * kCatStride);
+}
+
 template <bool kFull, typename Index>
-__device__ __forceinline__ void one_cell(const FuelConst *cat, const Inputs &in, const Outputs &out,
+__device__ __forceinline__ void one_cell(const float *cat, const Inputs &in, const Outputs &out,
                                          Index i) {
   const uint8_t code = __ldg(in.fuel + i);
   FireOut o{};
-  if (code < kMaxFuels && cat[code].has_fire != 0.0f) {
+  if (code < kMaxFuels && fuel_row(cat, code).has_fire != 0.0f) {
     const float m[5] = {__ldg(in.m[0] + i), __ldg(in.m[1] + i), __ldg(in.m[2] + i), __ldg(in.m[3] + i),
                         __ldg(in.m[4] + i)};
-    burn_cell<kFull>(cat[code], m, __ldg(in.ws + i), __ldg(in.waz + i), __ldg(in.slope + i),
-                     __ldg(in.aspect + i), o);
+    burn_cell<kFull>(fuel_row(cat, code), m, __ldg(in.ws + i), __ldg(in.waz + i),
+                     __ldg(in.slope + i), __ldg(in.aspect + i), o);
   }
   store_cell<kFull>(out, i, o);
 }
 
-// One cell per thread, grid-stride: every load and store is coalesced (4 or
-// 1 consecutive bytes per lane) and one copy of the cell code keeps the
-// kernel small in the instruction cache.  kFull: all ten fields; else the
-// three the propagation needs (the shared fields are the same operations,
-// so both give bit-identical values for them).
+// One cell per thread, grid-stride, cells [first, n): every load and store is
+// coalesced (4 or 1 consecutive bytes per lane).  kFull: all ten fields; else
+// the three the propagation needs (the shared fields are the same
+// operations, so both give the same values for them).
 // Index: uint32_t when n + the grid's threads fit in 32 bits (cheaper
 // address arithmetic), else uint64_t.
 template <bool kFull, typename Index>
-__global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, Index n) {
-  __shared__ FuelConst cat[kMaxFuels];
-  for (int t = threadIdx.x; t < (int)(sizeof(cat) / 4); t += blockDim.x)
-    reinterpret_cast<float *>(cat)[t] = reinterpret_cast<const float *>(c_catalog)[t];
-  __syncthreads();
+__global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, Index first, Index n) {
+  __shared__ float cat[kMaxFuels * kCatStride];
+  load_catalog(cat);
   const Index stride = (Index)gridDim.x * blockDim.x;
-  for (Index i = (Index)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+  for (Index i = first + (Index)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     one_cell<kFull>(cat, in, out, i);
 }
 
-// CTAs of fire_kernel<kFull, Index> resident per SM (registers limit it).
-template <bool kFull, typename Index>
-static int fire_ctas_per_sm(int threads) {
+// CTAs of a fire kernel resident per SM (registers limit it).
+template <typename K>
+static int ctas_per_sm(K kernel, int threads) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fire_kernel<kFull, Index>, threads, 0) !=
-          cudaSuccess ||
-      n < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1)
     n = 1;
   return n;
+}
+
+// one wave: as many CTAs as are resident at once, each striding over an
+// equal share (a second, partial wave would leave SMs idle at the end)
+static unsigned one_wave(uint64_t items, int threads, int sm_count, int per_sm) {
+  uint64_t blocks = (items + threads - 1) / threads;
+  const uint64_t cap = (uint64_t)sm_count * (uint64_t)per_sm;
+  if (blocks > cap) blocks = cap;
+  return blocks ? (unsigned)blocks : 1u;
 }
 
 template <bool kFull, typename Index>
 static cudaError_t launch_fire_t(const Inputs &in, const Outputs &out, uint64_t n, int sm_count,
                                  int threads, cudaStream_t stream) {
-  // one wave: as many CTAs as are resident at once, each striding over an
-  // equal share (a second, partial wave would leave SMs idle at the end)
-  uint64_t blocks = (n + threads - 1) / threads;
-  const uint64_t cap = (uint64_t)sm_count * (uint64_t)fire_ctas_per_sm<kFull, Index>(threads);
-  if (blocks > cap) blocks = cap;
-  if (blocks == 0) blocks = 1;
-  fire_kernel<kFull, Index><<<(unsigned)blocks, threads, 0, stream>>>(in, out, (Index)n);
+  auto k1 = fire_kernel<kFull, Index>;
+  k1<<<one_wave(n, threads, sm_count, ctas_per_sm(k1, threads)), threads, 0, stream>>>(in, out, (Index)0,
+                                                                                    (Index)n);
   return cudaGetLastError();
 }
 

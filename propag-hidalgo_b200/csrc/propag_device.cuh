@@ -102,8 +102,9 @@ __device__ __forceinline__ float pg_atan2f(float y, float x) {
 // Two arithmetics (`refm`, uniform per scenario):
 //   reference (refm = true, the default): the reference's own operations as
 //     nvcc compiles propag.cu with its default flags -- CUDA's atan2f and the
-//     __cosf intrinsic, and the two sums nvcc contracts into multiply-adds,
-//     dx*dx + dy*dy -> fma(dx, dx, dy*dy) and from.time + distance * rcp ->
+//     __cosf intrinsic, and the three sums nvcc contracts into multiply-adds,
+//     1.0 - e*cos -> fma(-e, cos, 1) (in float), dx*dx + dy*dy ->
+//     fma(dx, dx, dy*dy) and from.time + distance * rcp ->
 //     fma(distance, rcp, from.time).  A test compiles the reference's
 //     time_from from its source and checks these bits against it.
 //   portable (refm = false): the float cosine/arctangent above and every
@@ -115,8 +116,13 @@ struct Fire {
 
 __device__ __forceinline__ float spread_factor(float azimuth, const Fire &f, bool refm) {
   const float angle = fabsf(__fsub_rn(azimuth, f.azimuth_max));
-  const float p = __fmul_rn(f.eccentricity, refm ? __cosf(angle) : pg_cosf(angle));
-  const float denom = __double2float_rn(__dsub_rn(1.0, (double)p));
+  // denom = 1.0 - e * cos(angle): nvcc narrows the double subtraction of a
+  // float product to float (exact either way) and contracts it, so the
+  // reference computes fma(-e, cos, 1); the portable arithmetic rounds the
+  // product first
+  const float denom =
+      refm ? __fmaf_rn(-f.eccentricity, __cosf(angle), 1.0f)
+           : __double2float_rn(__dsub_rn(1.0, (double)__fmul_rn(f.eccentricity, pg_cosf(angle))));
   const double one_minus_e = __dsub_rn(1.0, (double)f.eccentricity);
   return __double2float_rn(__dmul_rn(one_minus_e, (double)__frcp_rd(denom)));
 }
@@ -153,10 +159,19 @@ __device__ __forceinline__ float time_from(int fx, int fy, float ftime, int tx, 
 
 // ---- DDA line-of-sight walk (propag.h:91-135) ------------------------------
 // Visits the cells from `from` to `to` inclusive in the reference's order and
-// reports whether one of them is a boundary.  The t-max accumulators are the
-// reference's float arithmetic: start 1/|d| (formed in double), step +1/|d|,
-// diagonal step when |tmax.x - tmax.y| < 1e-9.  The loop is bounded by
-// |dx| + |dy| + 2 visits, more than any walk takes.
+// reports whether one of them is a boundary; `steps` counts the cells
+// visited up to and including the first boundary.  The t-max accumulators
+// are the reference's float arithmetic: start 1/|d| (formed in double), step
+// +1/|d|, diagonal step when |tmax.x - tmax.y| < 1e-9 (a double comparison
+// in the reference: for a float v, (double)v < 1e-9 exactly when v is at most
+// the largest float below 1e-9).  The walk is bounded by |dx| + |dy| + 2
+// visits, more than any walk takes.
+//
+// The cells are generated kWalkBatch at a time by the (load-free) DDA
+// arithmetic, their bitmap words are loaded together, and then checked in
+// visiting order: one load latency per batch instead of one per cell.
+constexpr int kWalkBatch = 8;
+
 __device__ __forceinline__ bool is_boundary(const uint32_t *__restrict__ bnd, int64_t ix) {
   return (__ldg(bnd + (ix >> 5)) >> (ix & 31)) & 1u;
 }
@@ -168,34 +183,57 @@ __device__ __forceinline__ bool line_blocked(const uint32_t *__restrict__ bnd, i
   float tmx = __double2float_rn(1.0 / (double)(float)adx);
   float tmy = __double2float_rn(1.0 / (double)(float)ady);
   const float ddx = tmx, ddy = tmy;
+  const float kTie = __int_as_float(0x3089705F);  // the largest float below 1e-9
   int cx = fx, cy = fy;
-  const int limit = adx + ady + 2;
-  for (int n = 0; n < limit; ++n) {
-    const int px = cx, py = cy;
-    if (px == tx && py == ty) {
-      cx += sx;
-      cy += sy;
-    } else {
-      const bool vx = sx > 0 ? cx <= tx : cx >= tx;
-      const bool vy = sy > 0 ? cy <= ty : cy >= ty;
-      if (!(vx && vy)) return false;
-      if ((double)fabsf(__fsub_rn(tmx, tmy)) < 1e-9) {  // a double comparison, propag.h:122
-        cx += sx;
-        cy += sy;
-        tmx = __fadd_rn(tmx, ddx);
-        tmy = __fadd_rn(tmy, ddy);
-      } else if (tmx < tmy) {
-        cx += sx;
-        tmx = __fadd_rn(tmx, ddx);
-      } else {
-        cy += sy;
-        tmy = __fadd_rn(tmy, ddy);
+  int left = adx + ady + 2;  // visits the bound still allows
+  for (;;) {
+    uint32_t ix[kWalkBatch];  // cell index x + y W (grids below 2^32 cells)
+    int nv = 0;               // cells of this batch
+    bool ended = left <= 0;
+#pragma unroll
+    for (int i = 0; i < kWalkBatch; ++i) {
+      if (!ended && i < left) {
+        const int px = cx, py = cy;
+        if (px == tx && py == ty) {
+          cx += sx;
+          cy += sy;
+        } else {
+          const bool vx = sx > 0 ? cx <= tx : cx >= tx;
+          const bool vy = sy > 0 ? cy <= ty : cy >= ty;
+          if (!(vx && vy)) {
+            ended = true;
+          } else if (fabsf(__fsub_rn(tmx, tmy)) <= kTie) {
+            cx += sx;
+            cy += sy;
+            tmx = __fadd_rn(tmx, ddx);
+            tmy = __fadd_rn(tmy, ddy);
+          } else if (tmx < tmy) {
+            cx += sx;
+            tmx = __fadd_rn(tmx, ddx);
+          } else {
+            cy += sy;
+            tmy = __fadd_rn(tmy, ddy);
+          }
+        }
+        if (!ended) {
+          ix[i] = (uint32_t)px + (uint32_t)py * (uint32_t)W;
+          nv = i + 1;
+        }
       }
     }
-    ++steps;
-    if (is_boundary(bnd, (int64_t)px + (int64_t)py * W)) return true;
+    uint32_t word[kWalkBatch];
+#pragma unroll
+    for (int i = 0; i < kWalkBatch; ++i) word[i] = i < nv ? __ldg(bnd + (ix[i] >> 5)) : 0u;
+#pragma unroll
+    for (int i = 0; i < kWalkBatch; ++i) {
+      if (i < nv) {
+        ++steps;
+        if ((word[i] >> (ix[i] & 31)) & 1u) return true;
+      }
+    }
+    if (nv < kWalkBatch) return false;  // the walk ended in this batch
+    left -= kWalkBatch;
   }
-  return false;
 }
 
 // similar_fires (propag.cu:296-302): float differences compared against the

@@ -217,6 +217,7 @@ SIGNATURES = {
                                   C.c_void_p, C.c_int, C.POINTER(PropagOptions),
                                   C.POINTER(C.c_float)]),
     "propag_run_device_static": (C.c_int, [C.POINTER(PropagJob), C.c_void_p, C.POINTER(PropagStats)]),
+    "propag_static_last_status": (C.c_int, [C.c_void_p, C.POINTER(PropagStats)]),
     "propag_run_host": (C.c_int, [C.POINTER(Settings), C.POINTER(PropagTerrainPtrs),
                                   C.POINTER(PropagIgnition), C.c_uint64, C.POINTER(PropagOptions),
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PropagStats)]),

@@ -87,10 +87,13 @@ def test_reference_arith_equals_reference_source(pp, dx, dy):
     diff = got.view(np.uint32) != ref.view(np.uint32)
     assert not diff.any(), (f"{diff.sum()} of {diff.size} differ; first case {np.argmax(diff)}: "
                             f"{got[diff][:3]} vs {ref[diff][:3]}")
-    # the portable arithmetic is a different rounding of the same quantity
+    # the portable arithmetic is a different rounding of the same quantity:
+    # __cosf's absolute error (about 2^-21.4) grows by e / (1 - e cos) in
+    # the elliptical factor, up to 1000 times at e = 0.999
     port = _device_time_from(L, L.PROPAG_ARITH_PORTABLE, fx, fy, ftime, tx, ty, smax, az, ecc, dx, dy)
     rel = np.abs(port.astype(np.float64) - ref) / np.maximum(np.abs(ref.astype(np.float64)), 1e-30)
-    assert rel.max() < 1e-4
+    assert rel.max() < 1e-3
+    assert np.median(rel) < 1e-6
 
 
 @pytest.mark.parametrize("dx,dy", GRIDS[:2])

@@ -96,8 +96,8 @@ def test_fire_no_fuel_cells_are_zero(pp):
 
 
 def test_fire_unaligned_device_path(pp):
-    """Offset (non 16-byte aligned) device pointers take the scalar kernel and
-    give the same bits as the vector kernel."""
+    """Device pointers offset by one element (4-byte, not 16-byte aligned)
+    give the same bits as aligned ones."""
     import ctypes as C
     import torch
     from py_propag import _lib as L

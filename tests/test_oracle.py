@@ -226,3 +226,50 @@ def test_dda_walk_visits_from_to_inclusive(oracle, fx, fy, tx, ty):
     xs, ys = [c[0] for c in cells], [c[1] for c in cells]
     assert min(xs) >= min(fx, tx) and max(xs) <= max(fx, tx)
     assert min(ys) >= min(fy, ty) and max(ys) <= max(fy, ty)
+
+
+# Known answers of the reference's line walk (crates/geometry/src/lib.rs:
+# 508-649, the host DDA's tests): (from, to) -> cells visited.  The device
+# walk the propagation uses (crates/propag/src/propag.h:91-135, which the
+# oracle restates) visits the same cells on every one of them.
+DDA_KNOWN = [
+    ((0, 0), (0, 2), [(0, 0), (0, 1), (0, 2)]),
+    ((0, 0), (0, 1), [(0, 0), (0, 1)]),
+    ((0, 0), (0, -2), [(0, 0), (0, -1), (0, -2)]),
+    ((0, 0), (0, -1), [(0, 0), (0, -1)]),
+    ((0, 0), (2, 0), [(0, 0), (1, 0), (2, 0)]),
+    ((0, 0), (-2, 0), [(0, 0), (-1, 0), (-2, 0)]),
+    ((0, 0), (-2, -2), [(0, 0), (-1, -1), (-2, -2)]),
+    ((0, 0), (-2, 2), [(0, 0), (-1, 1), (-2, 2)]),
+    ((0, 0), (2, -2), [(0, 0), (1, -1), (2, -2)]),
+    ((0, 0), (1, -1), [(0, 0), (1, -1)]),
+    ((0, 0), (2, 2), [(0, 0), (1, 1), (2, 2)]),
+]
+
+
+@pytest.mark.parametrize("frm,to,cells", DDA_KNOWN)
+def test_dda_known_answers_of_the_reference(oracle, frm, to, cells):
+    got = [(int(a), int(b)) for a, b in oracle.dda_cells(frm[0], frm[1], to[0], to[1])]
+    assert got == cells
+
+
+def test_dda_special_case_propag(oracle):
+    """The reference's special_case_propag: the second cell of the walk from
+    (499, 99) to (500, 100) is (500, 100)."""
+    assert [tuple(int(v) for v in c) for c in oracle.dda_cells(499, 99, 500, 100)][1] == (500, 100)
+
+
+def test_dda_second_cell_is_the_neighbour_in_direction(oracle):
+    """The reference's neighbor_in_direction_same_as_line_to property
+    (crates/geometry/src/lib.rs:477-495, 511-521) on offsets within 300
+    cells: the walk's second cell is the neighbour in the direction of the
+    target (diagonal on |dx| = |dy|, else along the longer axis)."""
+    rng = np.random.default_rng(12)
+    for x, y in rng.integers(-300, 301, size=(4000, 2)):
+        x, y = int(x), int(y)
+        if x == 0 or y == 0:
+            continue
+        sx, sy = (x > 0) - (x < 0), (y > 0) - (y < 0)
+        want = (sx, sy) if abs(x) == abs(y) else ((sx, 0) if abs(x) > abs(y) else (0, sy))
+        got = tuple(int(v) for v in oracle.dda_cells(0, 0, x, y)[1])
+        assert got == want, (x, y, got, want)

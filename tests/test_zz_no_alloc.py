@@ -93,6 +93,10 @@ def test_static_equals_engine_on_consecutive_calls(pp):
 
 
 def test_static_allocates_no_device_memory(pp):
+    """Net device usage is unchanged by calls after the first (which takes
+    the scratch's address): free device memory before and after two calls is
+    the same.  This sees allocations still held at the end; the entry point's
+    source makes no cudaMalloc/cudaFree/cudaMallocHost call at all."""
     import torch
     from py_propag import _lib as L
     from py_propag import scenarios as S
@@ -125,3 +129,25 @@ def test_static_rejects_jobs_beyond_its_limits(pp):
     assert lib.propag_run_device_static(C.byref(j), None, None) == L.PROPAG_ERR_INVALID
     assert "does not fit" in L.last_error()
     assert lib.propag_run_device_static(None, None, None) == L.PROPAG_ERR_INVALID
+
+
+def test_static_status_without_stats(pp, monkeypatch):
+    """A caller that runs without `stats` (stream-ordered) reads the job's
+    outcome afterwards: a job stopped by the sweep limit (PROPAG_MAX_SWEEPS,
+    read at each call) reports it, and the next call clears it."""
+    from py_propag import _lib as L
+    from py_propag import scenarios as S
+    lib = L.lib()
+    sc = S.config0(size=96, seed=34)
+    job, keep = _device_job(pp, L, sc, 0)
+    monkeypatch.setenv("PROPAG_MAX_SWEEPS", "3")
+    assert lib.propag_run_device_static(C.byref(job), None, None) == 0, L.last_error()
+    st = L.PropagStats()
+    assert lib.propag_static_last_status(None, C.byref(st)) == L.PROPAG_ERR_TIMEOUT
+    assert st.status == 1 and "sweep limit" in L.last_error()
+    assert lib.propag_run_device_static(C.byref(job), None, C.byref(L.PropagStats())) == \
+        L.PROPAG_ERR_TIMEOUT
+    monkeypatch.delenv("PROPAG_MAX_SWEEPS")
+    assert lib.propag_run_device_static(C.byref(job), None, None) == 0, L.last_error()
+    assert lib.propag_static_last_status(None, C.byref(st)) == 0, L.last_error()
+    assert st.status == 0 and st.burned > 0
