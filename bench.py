@@ -54,13 +54,18 @@ FIRE_BYTES_PER_CELL = 49  # 37 B in (u8 fuel + 9 f32) + 12 B out (3 f32)
 # only) and identically by the CPU restatement in the same mode (full=2; same
 # schedule, bit-identical results).  The CPU legs time a bounded crop in that
 # mode and scale by it; the GPU leg reports whether its own count still agrees.
-WORK_EVALUATIONS = {"config1": 163564125}
+WORK_EVALUATIONS = {"config1": 163488517}
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # one single-pass ncu capture of the full-size workload; the command and the
 # figures are in profiles/dram_traffic_config1-4096.md.
 DRAM_TRAFFIC = {"config1": {"engine_kernel": 5.58e9 + 0.36089e9,
                             "fire_kernel": 557.95e6 + 181.74e6}}
+
+
+def _log(msg: str) -> None:
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
 
 
 def _peaks():
@@ -107,9 +112,10 @@ class Clocks:
 
     def __init__(self, index: int):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="propag_clocks_", suffix=".csv")
+        os.close(fd)
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={index}",
@@ -154,54 +160,93 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def _parallel(fn, terrain: dict, threads: int):
+    """Runs a CPU fire-behaviour function over the cells in `threads` slices
+    on as many threads (the ctypes calls release the GIL; every call builds
+    its own fuel catalog)."""
+    from concurrent.futures import ThreadPoolExecutor
+    n = next(iter(terrain.values())).size
+    cuts = np.linspace(0, n, threads + 1).astype(np.int64)
+    parts = [{k: np.ascontiguousarray(v.ravel()[a:b]) for k, v in terrain.items()}
+             for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(fn, parts))
+
+
 def cpu_baseline(sc, evaluations_full: int, threads: int, budget_s: float = 20.0,
                  use_firelib_c: bool = False) -> dict:
-    """Times the CPU path on a bounded sample of the workload: fire behaviour
-    on 1/16 of the cells (the reference's fireLib.c when asked and built,
-    else the FP64 restatement), propagation by the CPU restatement on a crop
-    around the first ignition, scaled by the full scenario's cell
-    evaluations."""
+    """Times the CPU path on this host's cores.
+
+    Fire behaviour: the reference's own fireLib.c when asked and built (else
+    the FP64 restatement) on a quarter of the workload's cells, on `threads`
+    threads, scaled to all cells.  Propagation (the reference has none on the
+    CPU): the CPU restatement of its kernel, in the engine's work-skipping
+    mode (same schedule and results as whole-tile sweeps), timed on a crop
+    of the workload around its first ignition and scaled by the full
+    workload's recorded cell evaluations (an extrapolation, labelled as one);
+    beside it, the whole 1024 x 1024 single-ignition scenario measured end to
+    end, and the evaluation rate of the reference's own whole-tile sweeps
+    (every cell of a tile in every sweep) on a 512 x 512 crop."""
     from oracle import oracle as O
-    t0 = time.perf_counter()
+    from py_propag import scenarios as S
     ncell = sc.width * sc.height
-    k = max(1, ncell // 16)
+    k = max(threads, ncell // 4)
     samp = {kk: np.ascontiguousarray(v.ravel()[:k]) for kk, v in sc.terrain.items()}
-    fire_kind = "fireLib.c (reference, 1 thread)" if use_firelib_c and O.have_firelib_c() else \
-        "FP64 restatement (1 thread)"
+    c_fire = use_firelib_c and O.have_firelib_c()
+    fire_kind = "fireLib.c (reference)" if c_fire else "FP64 restatement"
     tf = time.perf_counter()
-    if fire_kind.startswith("fireLib.c"):
-        O.burn_firelib_c(samp)
-    else:
-        O.burn_f64(samp)
+    _parallel(O.burn_firelib_c if c_fire else O.burn_f64, samp, threads)
     fire_s = (time.perf_counter() - tf) * (ncell / k)
-    crop = 256
+
+    def fire_fields(t):
+        f, _ = O.burn_f64(t)
+        return f[:, 4].astype(np.float32), f[:, 5].astype(np.float32), f[:, 6].astype(np.float32)
+
+    # the workload's own evaluation rate, on a 1024 x 1024 crop around its
+    # first ignition
+    crop = min(1024, sc.width, sc.height)
     cx, cy = sc.ignitions[0][0], sc.ignitions[0][1]
-    while True:
-        x0 = int(min(max(cx - crop // 2, 0), sc.width - crop))
-        y0 = int(min(max(cy - crop // 2, 0), sc.height - crop))
-        sub = {kk: np.ascontiguousarray(v[y0:y0 + crop, x0:x0 + crop]) for kk, v in sc.terrain.items()}
-        f, _ = O.burn_f64(sub)
-        ign = [(x - x0, y - y0, t) for (x, y, t) in sc.ignitions
-               if x0 <= x < x0 + crop and y0 <= y < y0 + crop]
-        tp = time.perf_counter()
-        r = O.propagate(crop, crop, sc.dx, sc.dy, sc.max_time, f[:, 4].astype(np.float32),
-                        f[:, 5].astype(np.float32), f[:, 6].astype(np.float32), ign,
-                        tile=323, threads=threads, full=2)
-        dt = time.perf_counter() - tp
-        prop_rate = r.stats["evaluations"] / dt
-        if time.perf_counter() - t0 > budget_s / 3 or crop >= 1024:
-            break
-        crop *= 2
+    x0 = int(min(max(cx - crop // 2, 0), sc.width - crop))
+    y0 = int(min(max(cy - crop // 2, 0), sc.height - crop))
+    sub = {kk: np.ascontiguousarray(v[y0:y0 + crop, x0:x0 + crop]) for kk, v in sc.terrain.items()}
+    sp, az, ec = fire_fields(sub)
+    ign = [(x - x0, y - y0, t) for (x, y, t) in sc.ignitions if x0 <= x < x0 + crop and y0 <= y < y0 + crop]
+    tp = time.perf_counter()
+    rc = O.propagate(crop, crop, sc.dx, sc.dy, sc.max_time, sp, az, ec, ign, tile=323,
+                     threads=threads, full=2, trig=2)
+    prop_rate = rc.stats["evaluations"] / (time.perf_counter() - tp)
     prop_s = evaluations_full / prop_rate
+    # the whole 1024 x 1024 single-ignition scenario, end to end
+    c0 = S.config0(size=1024)
+    sp, az, ec = fire_fields(c0.terrain)
+    tp = time.perf_counter()
+    r0 = O.propagate(c0.width, c0.height, c0.dx, c0.dy, c0.max_time, sp, az, ec, c0.ignitions,
+                     tile=323, threads=threads, full=2, trig=2)
+    c0_s = time.perf_counter() - tp
+    half = 512
+    x0 = y0 = int(c0.ignitions[0][0]) - half // 2
+    sub = {kk: np.ascontiguousarray(v[y0:y0 + half, x0:x0 + half]) for kk, v in c0.terrain.items()}
+    sp2, az2, ec2 = fire_fields(sub)
+    tp = time.perf_counter()
+    r1 = O.propagate(half, half, c0.dx, c0.dy, c0.max_time, sp2, az2, ec2,
+                     [(half // 2, half // 2, 0.0)], tile=323, threads=threads, full=1, trig=2)
+    full_rate = r1.stats["evaluations"] / (time.perf_counter() - tp)
     return {"value": 1.0 / (fire_s + prop_s), "unit": UNIT, "cores": threads,
             # the propagation (over 95 % of the time) is always the CPU restatement
             "kind": "port",
-            "sample": (f"fire behaviour: {fire_kind} on {k} of {ncell} cells, scaled; propagation: "
-                       f"CPU restatement of propag.cu (the reference has no CPU propagation) on a "
-                       f"{crop}x{crop} crop around the first ignition, {prop_rate:.3g} cell "
-                       f"evaluations/s on {threads} threads, scaled to the full scenario's "
-                       f"{evaluations_full} evaluations"),
-            "fire_s": fire_s, "propagation_s": prop_s}
+            "sample": (f"fire behaviour: {fire_kind} on {k} of {ncell} cells on {threads} threads, "
+                       f"scaled; propagation: CPU restatement of propag.cu (the reference has no CPU "
+                       f"propagation), {prop_rate:.3g} cell evaluations/s on {threads} threads "
+                       f"(work-skipping sweeps) timed on a {crop}x{crop} crop around the first "
+                       f"ignition and extrapolated to the full scenario's {evaluations_full} "
+                       f"evaluations"),
+            "fire_s": fire_s, "propagation_s": prop_s,
+            "config0_measured": {"value": 1.0 / c0_s, "unit": "scenarios/s (propagation only)",
+                                 "evaluations": r0.stats["evaluations"], "seconds": c0_s},
+            "reference_schedule": {"evaluations_per_s": full_rate,
+                                   "note": "whole-tile sweeps as the reference runs them (every cell "
+                                           "of the tile in every sweep), 512x512 crop of config 0; "
+                                           "same results, far more evaluations"}}
 
 
 def run_reference(args):
@@ -219,7 +264,7 @@ def run_reference(args):
     vals = []
     cb = None
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(sc, evals, threads, budget_s=10.0, use_firelib_c=True)
+        cb = cpu_baseline(sc, evals, threads, use_firelib_c=True)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = float(np.median(vals))
@@ -232,11 +277,14 @@ def run_reference(args):
 
 
 def serve_leg(lib, L, pp, dev, master, seconds: float, rate: float, budget_gb: float,
-              check: int = 8) -> dict:
+              check_every: int = 10, cap_requests: int = 1000) -> dict:
     """Serving loop: Poisson arrivals of window requests cut from a
     device-resident master terrain, submitted to a continuous-batching server
-    as they arrive; latency = submit to done (host clock).  A sample of the
-    requests is re-run alone through the plain path and compared bit for bit."""
+    as they arrive; latency = submit to done (host clock).  Every
+    `check_every`-th request's served arrival times are kept on the host, and
+    after the run the same requests are re-run alone through the plain path
+    and compared bit for bit.  Capacity: the first `cap_requests` requests
+    again, closed loop with 32 outstanding."""
     import torch
     from py_propag import scenarios as S
     from py_propag.batches import device_jobs
@@ -244,9 +292,23 @@ def serve_leg(lib, L, pp, dev, master, seconds: float, rate: float, budget_gb: f
     H, W = master["fuel_code"].shape
     mt = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in master.items()}
     prep = torch.cuda.Stream(dev)
-    srv = pp.Server(hbm_budget=int(budget_gb * 1e9), lanes=4, max_batch=64)
-    keep, res, sample = {}, {}, {}
-    check_ids = set(range(0, len(reqs), max(1, len(reqs) // check)))
+    torch.cuda.empty_cache()
+    free, _ = torch.cuda.mem_get_info(dev)
+    # the server reserves its budget up front; requests' own buffers (inputs,
+    # fire rasters, outputs) need room beside it
+    # (the server adds its slot scratch, about 2.6 GB, to the budget)
+    budget = int(max(min(budget_gb * 1e9, free - 45e9), 8e9))
+    srv = pp.Server(hbm_budget=budget, lanes=4, max_batch=64)
+    try:
+        return _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget,
+                      check_every, cap_requests, device_jobs)
+    finally:
+        srv.close()  # the dispatcher thread must stop before the process exits
+
+
+def _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget, check_every,
+           cap_requests, device_jobs):
+    keep, res, served = {}, {}, {}
 
     def make(i, r):
         n, x0, y0 = r["size"], r["x0"], r["y0"]
@@ -261,73 +323,81 @@ def serve_leg(lib, L, pp, dev, master, seconds: float, rate: float, budget_gb: f
         prep.synchronize()
         return jobs[0], terrains[0], kp
 
-    def collect(block=False):
+    def collect(block=False, check=True):
         for rid in list(keep):
-            out = srv.wait(rid, 600_000) if block else srv.poll(rid)
+            out = srv.wait(rid, 120_000) if block else srv.poll(rid)
+            if block and out is None:
+                raise RuntimeError(f"serving: request {rid} not done after 120 s")
             if out is not None:
                 res[rid] = out
-                if rid in check_ids:
-                    sample[rid] = keep[rid]
+                i = keep[rid][3]
+                if check and i % check_every == 0:
+                    served[i] = keep[rid][2][0][3].cpu().numpy()
                 del keep[rid]
                 srv.release(rid)
 
     t_start = time.perf_counter()
     ids = []
+    _log(f"serving: {len(reqs)} requests over {seconds:g} s, budget {budget / 1e9:.0f} GB")
     for i, r in enumerate(reqs):
         while time.perf_counter() - t_start < r["arrival"]:
             collect()
             time.sleep(0.0005)
+        if i % 500 == 0:
+            _log(f"serving: request {i}, {len(keep)} outstanding")
         job, terr, kp = make(i, r)
         rid = srv.submit(job, terr)
         ids.append(rid)
-        keep[rid] = (job, terr, kp, r)
+        keep[rid] = (job, terr, kp, i)
     collect(block=True)
     lat = np.array([(res[r]["done_ns"] - res[r]["submit_ns"]) / 1e6 for r in ids])
     span = (max(res[r]["done_ns"] for r in ids) - min(res[r]["submit_ns"] for r in ids)) / 1e9
-    # capacity: the same requests again, closed loop with 64 outstanding
-    check_ids.clear()
+    _log("serving: open loop done; capacity run")
+    # capacity: the first requests again, closed loop with 32 outstanding
     cap_ids = []
+    n_cap = min(len(reqs), cap_requests)
     t_cap = time.perf_counter()
-    for i, r in enumerate(reqs):
-        while len(keep) >= 64:
-            collect()
+    for i, r in enumerate(reqs[:n_cap]):
+        while len(keep) >= 32:
+            collect(check=False)
             time.sleep(0.0002)
         job, terr, kp = make(i, r)
         rid = srv.submit(job, terr)
         cap_ids.append(rid)
-        keep[rid] = (job, terr, kp, r)
-    collect(block=True)
-    capacity = len(reqs) / (time.perf_counter() - t_cap)
+        keep[rid] = (job, terr, kp, i)
+    collect(block=True, check=False)
+    capacity = n_cap / (time.perf_counter() - t_cap)
     cap_batch = float(np.mean([res[r]["batch_size"] for r in cap_ids]))
     srv.close()
-    # the sample alone through the plain path
+    _log(f"serving: capacity done; {len(served)} requests re-run alone")
+    # the checked requests alone through the plain path
     eng = lib.propag_engine_create(C.byref(L.PropagOptions(0, 0, 0, -1)))
     sptr = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     same = True
-    for rid, (job, terr, kp, r) in sample.items():
-        served = kp[0][3].clone()
-        kp[0][3].fill_(-1.0)
+    for i, times in served.items():
+        job, terr, kp = make(i, reqs[i])
         if lib.propag_fire_simple_device(job.width * job.height, C.byref(terr), job.speed_max,
                                          job.azimuth_max, job.eccentricity, sptr) or \
                 lib.propag_engine_run(eng, C.byref(job), 1, sptr, None):
             raise RuntimeError(L.last_error())
         torch.cuda.synchronize()
-        same &= bool(torch.equal(served, kp[0][3]))
+        same &= bool(np.array_equal(times.view(np.uint32), kp[0][3].cpu().numpy().view(np.uint32)))
+        del kp
     lib.propag_engine_destroy(eng)
     sizes = np.array([r["size"] for r in reqs])
     return {
         "workload": (f"config4: Poisson arrivals at {rate:g}/s for {seconds:g} s ({len(reqs)} requests), "
                      f"windows {sizes.min()}..{sizes.max()} square from a device-resident "
                      f"{W}x{H} master terrain, per-request wind/moisture/ignition, 1-12 h, "
-                     f"HBM budget {budget_gb:g} GB"),
+                     f"HBM budget {budget / 1e9:.0f} GB of engine scratch reserved by the server"),
         "value": len(reqs) / span, "unit": UNIT, "offered_rate": rate,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max())},
         "batch_size_mean": float(np.mean([res[r]["batch_size"] for r in ids])),
-        "capacity": {"value": capacity, "unit": UNIT, "batch_size_mean": cap_batch,
-                     "note": "same requests, closed loop with 64 outstanding (host wall clock, "
-                             "request preparation included)"},
-        "matches_plain_bitwise": same, "checked_alone": len(sample),
+        "capacity": {"value": capacity, "unit": UNIT, "batch_size_mean": cap_batch, "requests": n_cap,
+                     "note": "the first requests again, closed loop with 32 outstanding (host wall "
+                             "clock, request preparation included)"},
+        "matches_plain_bitwise": same, "checked_alone": len(served),
         "server": "4 streams, continuous batching (requests admitted while earlier batches run)",
     }
 
@@ -419,7 +489,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ensemble", type=int, default=256, help="members of the ensemble leg (0 = skip)")
     ap.add_argument("--uneven", type=int, default=64, help="scenarios of the uneven leg (0 = skip)")
-    ap.add_argument("--serve-seconds", type=float, default=30.0,
+    ap.add_argument("--serve-seconds", type=float, default=300.0,
                     help="length of the serving leg's arrival stream (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="serving arrivals per second")
     ap.add_argument("--plain-members", type=int, default=256,
@@ -527,6 +597,7 @@ def bench_b200(args):
 
     e2e = None
     if not args.no_e2e:
+        _log("end-to-end leg ...")
         e2e = e2e_leg(lib, L, pp, sc, args, world, dev, dev_time)
 
     peak, peak_kind = _peaks()
@@ -565,18 +636,22 @@ def bench_b200(args):
     del t_dev, fire, time_d, rx_d, ry_d, bnd_d
     if args.ensemble > 0:
         batch, bdesc = ensemble_batch(L, dev, args.ensemble)
+        _log("batched leg ...")
         line["batched"] = batched_leg(lib, L, pp, stream, batch, bdesc, args.steps, args.warmup,
                                       args.plain_members)
         del batch
     if args.uneven > 0:
         batch, bdesc = uneven_batch(L, dev, args.uneven)
+        _log("uneven batch leg ...")
         line["batched_uneven"] = batched_leg(lib, L, pp, stream, batch, bdesc, args.steps,
                                              args.warmup, args.uneven)
         del batch
     if args.serve_seconds > 0 and args.workload == "config1":
+        _log("serving leg ...")
         line["serving"] = serve_leg(lib, L, pp, dev, sc.terrain, args.serve_seconds, args.serve_rate,
                                     150.0)
     if rank == 0 and not args.no_cpu:
+        _log("CPU baseline ...")
         line["cpu_baseline"] = cpu_baseline(sc, stats["evaluations"], os.cpu_count() or 1)
     if world > 1:
         dist.barrier()

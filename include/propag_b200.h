@@ -128,6 +128,20 @@ typedef struct PropagWeatherPtrs {
 int propag_dmoist_device(uint64_t n, int hour, int month, const PropagWeatherPtrs *weather,
                          const float *slope, const float *aspect, const uint8_t *fuel,
                          float scale, float *d1hr, float *d10hr, float *d100hr, void *stream);
+/* Dead fuel moisture and fire behaviour fused into one pass: per cell the
+ * dmoist model at `hour` of `month` from the cell's weather (as
+ * propag_dmoist_device with scale 0.01), then the three fields the
+ * propagation needs (as propag_fire_simple_device), with no moisture
+ * rasters written or read in between.  terrain's d1hr/d10hr/d100hr are not
+ * read (may be NULL); the other nine rasters are.  Same bits as the two
+ * passes in a row.  Device pointers, stream-ordered.  Fuses the moisture
+ * of crates/dmoist/src/lib.rs:55-137 ahead of cuda_standard_simple_burn
+ * (crates/firelib/src/cuda.rs:57-95), which the reference runs apart (its
+ * moisture comes from host scalars). */
+int propag_fire_weather_device(uint64_t n, int hour, int month, const PropagWeatherPtrs *weather,
+                               const PropagTerrainPtrs *terrain, float *speed_max,
+                               float *azimuth_max, float *eccentricity, void *stream);
+
 /* Same over host buffers (copies in and out, synchronises). */
 int propag_dmoist_host(uint64_t n, int hour, int month, const PropagWeatherPtrs *weather,
                        const float *slope, const float *aspect, const uint8_t *fuel, float scale,
@@ -255,6 +269,12 @@ typedef struct PropagJob {
 typedef struct propag_engine propag_engine;
 
 propag_engine *propag_engine_create(const PropagOptions *opt);
+
+/* Device scratch the engine holds for one job of width x height cells
+ * (references, referrer boxes, travel-time planes, second state copy,
+ * boundary and pending bitmaps: about 60 bytes per cell), as a run lays it
+ * out; the server admits requests by it.  No counterpart in the reference. */
+uint64_t propag_engine_job_bytes(uint32_t width, uint32_t height);
 void propag_engine_destroy(propag_engine *engine);
 
 /* Propagates n_jobs scenarios in one persistent launch.  Stream-ordered; the
@@ -281,14 +301,22 @@ int propag_engine_last_stats(propag_engine *engine, void *stream, PropagStats *s
  * pointers, like PropagJob; `terrain` optional: with it the fire pass runs
  * first and writes the job's fire rasters).  Whenever a lane is free the
  * dispatcher takes the requests waiting at that moment, up to max_batch and
- * within hbm_budget bytes of device memory in flight (each request counts
- * `device_bytes`, 96 B per cell when 0), and runs them as one batch on that
- * lane; requests that arrive while batches are on the GPU are admitted as
- * lanes and memory free up, and run alongside them.  A request's results are
+ * within hbm_budget bytes of engine scratch in flight (each request counts
+ * `device_bytes`, propag_engine_job_bytes when 0), and runs them as one batch
+ * on that lane; requests that arrive while batches are on the GPU are
+ * admitted as lanes and memory free up, and run alongside them (a request
+ * of 2048 x 2048 cells or more runs in a batch of its own, on the largest
+ * clusters).  With a
+ * budget, each lane reserves hbm_budget / lanes of engine scratch when the
+ * server is created (plus slot scratch, about 10 MB per job of a batch, and
+ * pinned staging), so that serving itself allocates and frees no device
+ * memory; a request larger than a lane's share fails with PROPAG_ERR_OOM.
+ * A request's results are
  * the same alone and in any batch.  No counterpart in the reference (one
  * synchronous propagation per call, crates/propag/src/propag.rs:323-574). */
 typedef struct PropagServerOptions {
-  uint64_t hbm_budget; /* bytes of device memory in flight; 0 = no limit */
+  uint64_t hbm_budget; /* bytes of engine scratch in flight, reserved at creation;
+                          0 = no limit (scratch grows on demand) */
   uint32_t lanes;      /* batches in flight at once (streams); 0 = 4 */
   uint32_t max_batch;  /* requests per batch; 0 = 64 */
   int32_t device;      /* CUDA device ordinal; -1 = the current device */

@@ -41,6 +41,12 @@ cudaError_t launch_engine(const JobDev *jobs, uint32_t n_jobs, const SlotDev *sl
 cudaError_t engine_max_clusters(int csize, int threads, size_t smem, int *n);
 cudaError_t launch_post(const JobDev *jobs, uint32_t n_jobs, uint64_t max_cells, int sms,
                         StatsDev *stats, cudaStream_t stream);
+cudaError_t launch_fire_weather(uint64_t n, int hour, int month, const float *t, const float *rh,
+                                const float *cc, const float *pp, const uint8_t *fuel,
+                                const float *herb, const float *wood, const float *ws,
+                                const float *waz, const float *slope, const float *aspect,
+                                float *speed_max, float *azimuth_max, float *eccentricity,
+                                int sm_count, cudaStream_t stream);
 // selftest.cu
 cudaError_t launch_time_from(bool refm, uint64_t n, const int32_t *fx, const int32_t *fy,
                              const float *ftime, const int32_t *tx, const int32_t *ty,
@@ -105,8 +111,9 @@ struct DevBuf {
   ~DevBuf() {
     if (p) cudaFree(p);
   }
-  // Grows to at least `bytes`.  Growth waits for `stream` first.
-  cudaError_t reserve(size_t bytes, cudaStream_t stream) {
+  // Grows to at least `bytes` (with 1/8 headroom for the next growth unless
+  // `exact`).  Growth waits for `stream` first.
+  cudaError_t reserve(size_t bytes, cudaStream_t stream, bool exact = false) {
     if (bytes <= cap) return cudaSuccess;
     if (p) {
       cudaError_t e = cudaStreamSynchronize(stream);
@@ -115,7 +122,7 @@ struct DevBuf {
       p = nullptr;
       cap = 0;
     }
-    const size_t want = bytes + bytes / 8 + 256;
+    const size_t want = exact ? bytes + 256 : bytes + bytes / 8 + 256;
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) return e;
     cap = want;
@@ -180,7 +187,41 @@ namespace propag {
 // lanes) keep to clusters: a group-mode launch is cooperative and occupies
 // every SM, so its teams would wait for CTAs that other kernels hold.
 void engine_keep_to_clusters(propag_engine *e) { e->auto_groups = false; }
+
+
+// Reserves the engine's device scratch and pinned staging for batches of up
+// to max_jobs jobs whose job scratch sums to at most job_bytes, with slot
+// scratch of slot_bytes, so that such batches allocate nothing (a later
+// larger batch still grows the buffers).
+int engine_reserve(propag_engine *e, size_t job_bytes, uint32_t max_jobs, size_t slot_bytes,
+                   cudaStream_t stream) {
+  CK(cudaSetDevice(e->device));
+  CK(e->job_scratch.reserve(job_bytes, stream, true));
+  CK(e->slot_scratch.reserve(slot_bytes, stream, true));
+  CK(e->meta.reserve(align_up(sizeof(JobDev) * max_jobs, 256) + align_up(sizeof(SlotDev) * max_jobs, 256) +
+                         align_up(sizeof(StatsDev) * max_jobs, 256) + 256 +
+                         align_up(sizeof(uint32_t) * max_jobs, 256),
+                     stream));
+  if (e->pinned_jobs < max_jobs) {
+    if (e->jobs_pinned) cudaFreeHost(e->jobs_pinned);
+    e->jobs_pinned = nullptr;
+    CK(cudaMallocHost(&e->jobs_pinned, sizeof(JobDev) * max_jobs + sizeof(uint32_t) * max_jobs));
+    e->pinned_jobs = max_jobs;
+  }
+  if (e->pinned_slots < max_jobs) {
+    if (e->slots_pinned) cudaFreeHost(e->slots_pinned);
+    e->slots_pinned = nullptr;
+    CK(cudaMallocHost(&e->slots_pinned, sizeof(SlotDev) * max_jobs));
+    e->pinned_slots = max_jobs;
+  }
+  return PROPAG_OK;
+}
 }  // namespace propag
+
+extern "C" uint64_t propag_engine_job_bytes(uint32_t width, uint32_t height) {
+  const uint64_t N = (uint64_t)width * height, words = (N + 31) / 32;
+  return align_up(N * 4, 256) * 15 + 2 * align_up(words * 4, 256);
+}
 
 extern "C" propag_engine *propag_engine_create(const PropagOptions *opt) {
   int sms = 0;
@@ -1057,6 +1098,31 @@ extern "C" int propag_slope_aspect_device(uint32_t width, uint32_t height, doubl
     return fail(PROPAG_ERR_INVALID, "invalid pixel size");
   if (!dem || !slope || !aspect) return fail(PROPAG_ERR_INVALID, "null raster");
   CK(launch_slope_aspect((int)width, (int)height, dx, dy, dem, slope, aspect, sms, (cudaStream_t)stream));
+  return PROPAG_OK;
+}
+
+// =============================================== moisture + fire behaviour ==
+extern "C" int propag_fire_weather_device(uint64_t n, int hour, int month,
+                                          const PropagWeatherPtrs *weather,
+                                          const PropagTerrainPtrs *terrain, float *speed_max,
+                                          float *azimuth_max, float *eccentricity, void *stream) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (!weather || !terrain || !speed_max || !azimuth_max || !eccentricity)
+    return fail(PROPAG_ERR_INVALID, "null argument");
+  if (hour < 0 || hour > 23 || month < 1 || month > 12)
+    return fail(PROPAG_ERR_INVALID, "hour must be 0..23 and month 1..12");
+  if (n == 0) return PROPAG_OK;
+  if (!weather->temperature || !weather->humidity || !weather->cloud_cover || !weather->precipitation)
+    return fail(PROPAG_ERR_INVALID, "null weather raster");
+  const PropagTerrainPtrs &t = *terrain;
+  if (!t.fuel_code || !t.herb || !t.wood || !t.wind_speed || !t.wind_azimuth || !t.slope || !t.aspect)
+    return fail(PROPAG_ERR_INVALID, "null terrain raster");
+  CK(launch_fire_weather(n, hour, month, weather->temperature, weather->humidity, weather->cloud_cover,
+                         weather->precipitation, t.fuel_code, t.herb, t.wood, t.wind_speed,
+                         t.wind_azimuth, t.slope, t.aspect, speed_max, azimuth_max, eccentricity, sms,
+                         (cudaStream_t)stream));
   return PROPAG_OK;
 }
 

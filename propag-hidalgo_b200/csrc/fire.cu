@@ -45,6 +45,7 @@
 #include <cstdint>
 
 #include "catalog.hpp"
+#include "dmoist_device.cuh"
 
 namespace propag {
 
@@ -280,6 +281,35 @@ __global__ void __launch_bounds__(256) fire_kernel(Inputs in, Outputs out, Index
     one_cell<kFull>(cat, in, out, i);
 }
 
+// Dead fuel moisture and fire behaviour in one pass (no d1/d10/d100 rasters
+// in between): per cell the dmoist model at `hour` from the cell's weather
+// (dmoist_cell, percent values scaled to fractions as the moisture pass's
+// scale 0.01 does), then the three fields the propagation needs.  The same
+// operations as the moisture pass followed by fire_kernel<false>, so the
+// same bits.  Cells without fire skip the moisture model (their outputs are
+// 0 either way).
+template <typename Index>
+__global__ void __launch_bounds__(256) fire_weather_kernel(DmoistIn win, int hour, int month,
+                                                           Inputs in, Outputs out, Index n) {
+  __shared__ float cat[kMaxFuels * kCatStride];
+  __shared__ DmoistTables T;
+  load_dmoist_tables(T);
+  load_catalog(cat);
+  const Index stride = (Index)gridDim.x * blockDim.x;
+  for (Index i = (Index)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint8_t code = __ldg(in.fuel + i);
+    FireOut o{};
+    if (code < kMaxFuels && fuel_row(cat, code).has_fire != 0.0f) {
+      const float slope = __ldg(in.slope + i), aspect = __ldg(in.aspect + i);
+      float m1, m10, m100;
+      dmoist_cell(T, win, (uint64_t)n, (uint64_t)i, hour, month, code, slope, aspect, m1, m10, m100);
+      const float m[5] = {m1 * 0.01f, m10 * 0.01f, m100 * 0.01f, __ldg(in.m[3] + i), __ldg(in.m[4] + i)};
+      burn_cell<false>(fuel_row(cat, code), m, __ldg(in.ws + i), __ldg(in.waz + i), slope, aspect, o);
+    }
+    store_cell<false>(out, i, o);
+  }
+}
+
 // CTAs of a fire kernel resident per SM (registers limit it).
 template <typename K>
 static int ctas_per_sm(K kernel, int threads) {
@@ -339,6 +369,33 @@ cudaError_t launch_fire(bool full, uint64_t n, const uint8_t *fuel, const float 
                   : launch_fire_t<true, uint64_t>(in, out, n, sm_count, threads, stream);
   return narrow ? launch_fire_t<false, uint32_t>(in, out, n, sm_count, threads, stream)
                 : launch_fire_t<false, uint64_t>(in, out, n, sm_count, threads, stream);
+}
+
+cudaError_t launch_fire_weather(uint64_t n, int hour, int month, const float *t, const float *rh,
+                                const float *cc, const float *pp, const uint8_t *fuel,
+                                const float *herb, const float *wood, const float *ws,
+                                const float *waz, const float *slope, const float *aspect,
+                                float *speed_max, float *azimuth_max, float *eccentricity,
+                                int sm_count, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  DmoistIn win{t, rh, cc, pp, slope, aspect, fuel};
+  Inputs in{fuel, {nullptr, nullptr, nullptr, herb, wood}, ws, waz, slope, aspect};
+  Outputs out{};
+  out.f[4] = speed_max;
+  out.f[5] = azimuth_max;
+  out.f[6] = eccentricity;
+  const int threads = 256;
+  const bool narrow = n + (uint64_t)sm_count * 8 * threads < (1ull << 32);
+  if (narrow) {
+    auto k = fire_weather_kernel<uint32_t>;
+    k<<<one_wave(n, threads, sm_count, ctas_per_sm(k, threads)), threads, 0, stream>>>(
+        win, hour, month, in, out, (uint32_t)n);
+  } else {
+    auto k = fire_weather_kernel<uint64_t>;
+    k<<<one_wave(n, threads, sm_count, ctas_per_sm(k, threads)), threads, 0, stream>>>(
+        win, hour, month, in, out, (uint64_t)n);
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace propag

@@ -31,8 +31,21 @@
 
 namespace propag {
 void engine_keep_to_clusters(propag_engine *e);  // api.cpp
+int engine_reserve(propag_engine *e, size_t job_bytes, uint32_t max_jobs, size_t slot_bytes,
+                   cudaStream_t stream);
 }
 using propag::engine_keep_to_clusters;
+using propag::engine_reserve;
+
+// Slot scratch a lane reserves per job of a batch: dirty bitmaps, update
+// arrays and list overflow of one team for tiles up to the default 323 x 323
+// (about 9 MB in the worst cluster size).
+constexpr size_t kSlotBytesPerJob = 10u << 20;
+
+// Requests of at least this many cells run in a batch of their own: a batch
+// of many jobs gets small clusters (as many jobs at once as fit), and a
+// large job on a small cluster would hold its lane for seconds.
+constexpr uint64_t kAloneCells = 2048ull * 2048ull;
 
 namespace {
 
@@ -55,6 +68,7 @@ struct Lane {
   propag_engine *eng = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  uint64_t cap = 0;          // job scratch reserved at start-up (0: grown on demand)
   std::vector<int64_t> ids;  // requests of the batch in flight (empty: free)
 };
 
@@ -109,25 +123,30 @@ bool propag_server::dispatch(Lane &lane) {
   std::vector<bool> has;
   {
     std::lock_guard<std::mutex> lk(mu);
+    uint64_t lane_bytes = 0;
     while (!pending.empty() && ids.size() < max_batch) {
       Request &r = reqs[pending.front()];
-      if (budget && in_use + r.bytes > budget) {
-        if (in_use == 0 && ids.empty()) {  // can never fit: fail it
-          r.res.status = PROPAG_ERR_OOM;
-          r.message = "request needs more device memory than the server's budget";
-          pending.pop_front();
-          cv_done.notify_all();
-          continue;
-        }
-        break;
+      if ((lane.cap && r.bytes > lane.cap) || (budget && r.bytes > budget)) {
+        // can never fit: fail it
+        r.res.status = PROPAG_ERR_OOM;
+        r.message = "request needs more device memory than the server's budget";
+        pending.pop_front();
+        cv_done.notify_all();
+        continue;
       }
+      // a lane's batch fits the scratch it reserved at start-up
+      if ((budget && in_use + r.bytes > budget) || (lane.cap && lane_bytes + r.bytes > lane.cap)) break;
+      const bool large = (uint64_t)r.job.width * r.job.height >= kAloneCells;
+      if (large && !ids.empty()) break;  // it starts the next batch, alone
       in_use += r.bytes;
+      lane_bytes += r.bytes;
       r.res.start_ns = now_ns();
       ids.push_back(pending.front());
       jobs.push_back(r.job);
       terr.push_back(r.terrain);
       has.push_back(r.has_terrain);
       pending.pop_front();
+      if (large) break;
     }
     for (int64_t id : ids) reqs[id].res.batch_size = (uint32_t)ids.size();
   }
@@ -203,6 +222,25 @@ extern "C" propag_server *propag_server_create(const PropagServerOptions *opt) {
     s->lanes.push_back(lane);
   }
   cudaGetDevice(&s->device);
+  // With a budget, every lane reserves its share of it up front as job
+  // scratch, plus slot scratch and staging for max_batch jobs, so that
+  // serving allocates and frees no device memory: a cudaFree waits for the
+  // whole device and would stall the other lanes' batches.
+  if (s->budget) {
+    for (Lane &l : s->lanes) {
+      l.cap = s->budget / n_lanes;
+      if (engine_reserve(l.eng, l.cap, s->max_batch, kSlotBytesPerJob * s->max_batch, l.stream) != PROPAG_OK ||
+          cudaStreamSynchronize(l.stream) != cudaSuccess) {
+        for (Lane &m : s->lanes) {
+          cudaStreamDestroy(m.stream);
+          cudaEventDestroy(m.done);
+          propag_engine_destroy(m.eng);
+        }
+        delete s;
+        return nullptr;
+      }
+    }
+  }
   s->worker = std::thread([s] { s->run(); });
   return s;
 }
@@ -219,10 +257,8 @@ extern "C" int64_t propag_server_submit(propag_server *s, const PropagJob *job,
     r.terrain = *terrain;
     r.has_terrain = true;
   }
-  // engine scratch (references and referrer boxes 20 B, travel times 32 B,
-  // boundary bits) + fire rasters 12 B + outputs 8 B per cell, when the
-  // caller does not say
-  r.bytes = device_bytes ? device_bytes : (uint64_t)job->width * job->height * 96u;
+  // the engine scratch the request takes, when the caller does not say
+  r.bytes = device_bytes ? device_bytes : propag_engine_job_bytes(job->width, job->height);
   r.res.submit_ns = now_ns();
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return PROPAG_ERR_INVALID;

@@ -23,7 +23,6 @@ PROPAG_TILE_WHOLE_GRID = -1
 PROPAG_CLUSTER_GROUPS = -1  # PropagOptions.cluster: teams of CTAs over the whole device
 PROPAG_ARITH_REFERENCE = 0  # time_from with the reference's operations (CUDA atan2f, __cosf, contracted)
 PROPAG_ARITH_PORTABLE = 1   # time_from with portable operations a CPU reproduces bit for bit
-SERVER_DEFAULT_BYTES_PER_CELL = 96  # a request's device memory when submit gets 0
 
 
 class GT(C.Structure):
@@ -183,6 +182,7 @@ SIGNATURES = {
     "propag_fire_full_host": (C.c_int, [C.c_uint64, C.POINTER(PropagTerrainPtrs),
                                         C.POINTER(PropagFireFields)]),
     "propag_engine_create": (C.c_void_p, [C.POINTER(PropagOptions)]),
+    "propag_engine_job_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32]),
     "propag_engine_destroy": (None, [C.c_void_p]),
     "propag_engine_run": (C.c_int, [C.c_void_p, C.POINTER(PropagJob), C.c_uint32, C.c_void_p,
                                     C.POINTER(PropagStats)]),
@@ -197,6 +197,9 @@ SIGNATURES = {
     "propag_dmoist_device": (C.c_int, [C.c_uint64, C.c_int, C.c_int, C.POINTER(PropagWeatherPtrs),
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p]),
+    "propag_fire_weather_device": (C.c_int, [C.c_uint64, C.c_int, C.c_int, C.POINTER(PropagWeatherPtrs),
+                                             C.POINTER(PropagTerrainPtrs), C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]),
     "propag_dmoist_host": (C.c_int, [C.c_uint64, C.c_int, C.c_int, C.POINTER(PropagWeatherPtrs),
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p,
                                      C.c_void_p, C.c_void_p]),

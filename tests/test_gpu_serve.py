@@ -60,8 +60,10 @@ def test_budget_and_bad_requests(pp):
     from py_propag import _lib as L
     scs = _uneven(n=2, seed=53)
     jobs, terrains, keep = _device_batch(pp, L, scs, [0, 0])
-    small = min(sc.width * sc.height for sc in scs) * L.SERVER_DEFAULT_BYTES_PER_CELL
-    srv = pp.Server(hbm_budget=small, lanes=2)
+    # each of the two lanes reserves half the budget: room for the smaller
+    # request's engine scratch, not the larger one's
+    small = min(L.lib().propag_engine_job_bytes(sc.width, sc.height) for sc in scs)
+    srv = pp.Server(hbm_budget=2 * small, lanes=2)
     big = int(np.argmax([sc.width * sc.height for sc in scs]))
     rid = srv.submit(jobs[big], terrains[big])
     with pytest.raises(pp.PropagCudaError, match="budget"):
