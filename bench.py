@@ -338,11 +338,16 @@ def _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget,
 
     t_start = time.perf_counter()
     ids = []
+    overloaded = None
     _log(f"serving: {len(reqs)} requests over {seconds:g} s, budget {budget / 1e9:.0f} GB")
     for i, r in enumerate(reqs):
         while time.perf_counter() - t_start < r["arrival"]:
             collect()
             time.sleep(0.0005)
+        if len(keep) > 256:  # the server falls behind the arrivals: stop offering
+            overloaded = i
+            _log(f"serving: {len(keep)} requests outstanding at request {i}; arrivals stopped")
+            break
         if i % 500 == 0:
             _log(f"serving: request {i}, {len(keep)} outstanding")
         job, terr, kp = make(i, r)
@@ -350,6 +355,7 @@ def _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget,
         ids.append(rid)
         keep[rid] = (job, terr, kp, i)
     collect(block=True)
+    n_req = len(ids)
     lat = np.array([(res[r]["done_ns"] - res[r]["submit_ns"]) / 1e6 for r in ids])
     span = (max(res[r]["done_ns"] for r in ids) - min(res[r]["submit_ns"] for r in ids)) / 1e9
     _log("serving: open loop done; capacity run")
@@ -386,11 +392,13 @@ def _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget,
     lib.propag_engine_destroy(eng)
     sizes = np.array([r["size"] for r in reqs])
     return {
-        "workload": (f"config4: Poisson arrivals at {rate:g}/s for {seconds:g} s ({len(reqs)} requests), "
+        "workload": (f"config4: Poisson arrivals at {rate:g}/s for {seconds:g} s ({n_req} requests"
+                     + (f", stopped early: the server fell behind" if overloaded is not None else "")
+                     + "), "
                      f"windows {sizes.min()}..{sizes.max()} square from a device-resident "
                      f"{W}x{H} master terrain, per-request wind/moisture/ignition, 1-12 h, "
                      f"HBM budget {budget / 1e9:.0f} GB of engine scratch reserved by the server"),
-        "value": len(reqs) / span, "unit": UNIT, "offered_rate": rate,
+        "value": n_req / span, "unit": UNIT, "offered_rate": rate,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max())},
         "batch_size_mean": float(np.mean([res[r]["batch_size"] for r in ids])),

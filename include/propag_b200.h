@@ -304,9 +304,7 @@ int propag_engine_last_stats(propag_engine *engine, void *stream, PropagStats *s
  * within hbm_budget bytes of engine scratch in flight (each request counts
  * `device_bytes`, propag_engine_job_bytes when 0), and runs them as one batch
  * on that lane; requests that arrive while batches are on the GPU are
- * admitted as lanes and memory free up, and run alongside them (a request
- * of 2048 x 2048 cells or more runs in a batch of its own, on the largest
- * clusters).  With a
+ * admitted as lanes and memory free up, and run alongside them.  With a
  * budget, each lane reserves hbm_budget / lanes of engine scratch when the
  * server is created (plus slot scratch, about 10 MB per job of a batch, and
  * pinned staging), so that serving itself allocates and frees no device

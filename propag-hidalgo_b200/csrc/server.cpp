@@ -42,11 +42,6 @@ using propag::engine_reserve;
 // (about 9 MB in the worst cluster size).
 constexpr size_t kSlotBytesPerJob = 10u << 20;
 
-// Requests of at least this many cells run in a batch of their own: a batch
-// of many jobs gets small clusters (as many jobs at once as fit), and a
-// large job on a small cluster would hold its lane for seconds.
-constexpr uint64_t kAloneCells = 2048ull * 2048ull;
-
 namespace {
 
 uint64_t now_ns() {
@@ -136,8 +131,6 @@ bool propag_server::dispatch(Lane &lane) {
       }
       // a lane's batch fits the scratch it reserved at start-up
       if ((budget && in_use + r.bytes > budget) || (lane.cap && lane_bytes + r.bytes > lane.cap)) break;
-      const bool large = (uint64_t)r.job.width * r.job.height >= kAloneCells;
-      if (large && !ids.empty()) break;  // it starts the next batch, alone
       in_use += r.bytes;
       lane_bytes += r.bytes;
       r.res.start_ns = now_ns();
@@ -146,7 +139,6 @@ bool propag_server::dispatch(Lane &lane) {
       terr.push_back(r.terrain);
       has.push_back(r.has_terrain);
       pending.pop_front();
-      if (large) break;
     }
     for (int64_t id : ids) reqs[id].res.batch_size = (uint32_t)ids.size();
   }
