@@ -59,8 +59,8 @@ WORK_EVALUATIONS = {"config1": 163488517}
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # one single-pass ncu capture of the full-size workload; the command and the
 # figures are in profiles/dram_traffic_config1-4096.md.
-DRAM_TRAFFIC = {"config1": {"engine_kernel": 5.58e9 + 0.36089e9,
-                            "fire_kernel": 557.95e6 + 181.74e6}}
+DRAM_TRAFFIC = {"config1": {"engine_kernel": 988.88e6 + 348.53e6,
+                            "fire_kernel": 558.02e6 + 181.39e6}}
 
 
 def _log(msg: str) -> None:
@@ -344,7 +344,7 @@ def _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget,
         while time.perf_counter() - t_start < r["arrival"]:
             collect()
             time.sleep(0.0005)
-        if len(keep) > 256:  # the server falls behind the arrivals: stop offering
+        if len(keep) > 64:  # the server falls behind the arrivals: stop offering
             overloaded = i
             _log(f"serving: {len(keep)} requests outstanding at request {i}; arrivals stopped")
             break
@@ -393,7 +393,8 @@ def _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget,
     sizes = np.array([r["size"] for r in reqs])
     return {
         "workload": (f"config4: Poisson arrivals at {rate:g}/s for {seconds:g} s ({n_req} requests"
-                     + (f", stopped early: the server fell behind" if overloaded is not None else "")
+                     + (f" of {len(reqs)}: arrivals stopped when 64 requests were outstanding"
+                        if overloaded is not None else "")
                      + "), "
                      f"windows {sizes.min()}..{sizes.max()} square from a device-resident "
                      f"{W}x{H} master terrain, per-request wind/moisture/ignition, 1-12 h, "
@@ -406,6 +407,7 @@ def _serve(srv, lib, L, torch, dev, reqs, mt, prep, W, H, seconds, rate, budget,
                      "note": "the first requests again, closed loop with 32 outstanding (host wall "
                              "clock, request preparation included)"},
         "matches_plain_bitwise": same, "checked_alone": len(served),
+        "fell_behind_at_s": (None if overloaded is None else float(reqs[overloaded]["arrival"])),
         "server": "4 streams, continuous batching (requests admitted while earlier batches run)",
     }
 
