@@ -499,8 +499,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ensemble", type=int, default=256, help="members of the ensemble leg (0 = skip)")
     ap.add_argument("--uneven", type=int, default=64, help="scenarios of the uneven leg (0 = skip)")
-    ap.add_argument("--serve-seconds", type=float, default=300.0,
+    ap.add_argument("--serve-seconds", type=float, default=90.0,
                     help="length of the serving leg's arrival stream (0 = skip)")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run the serving leg alone and print its JSON object (the main run "
+                         "starts it so, in a child process with a time limit)")
+    ap.add_argument("--serve-terrain", default="",
+                    help="with --serve-only: .npz of the master terrain (else it is generated)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="serving arrivals per second")
     ap.add_argument("--plain-members", type=int, default=256,
                     help="ensemble members timed one by one on the plain path")
@@ -509,7 +514,47 @@ def main():
         return run_reference(args)
     if args.warmup < 0 or args.steps < 1:
         raise SystemExit("--steps >= 1 and --warmup >= 0")
+    if args.serve_only:
+        return serve_only(args)
     bench_b200(args)
+
+
+def serve_only(args):
+    """The serving leg on its own (config 4 on the 4096^2 master terrain)."""
+    import torch
+
+    import py_propag as pp
+    from py_propag import _lib as L
+    from py_propag import scenarios as S
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if args.serve_terrain:
+        with np.load(args.serve_terrain) as z:
+            master = {k: z[k] for k in z.files}
+    else:
+        master = S.config1(size=4096).terrain
+    res = serve_leg(L.lib(), L, pp, dev, master, args.serve_seconds, args.serve_rate, 150.0)
+    print(json.dumps(res), flush=True)
+
+
+def serving_child(args, terrain: dict) -> dict:
+    """Runs the serving leg in a child process with a time limit, so that a
+    server that falls behind its arrivals (config 4's windows reach 4096^2,
+    a quarter of them 2048^2 or more) cannot stall the benchmark."""
+    import tempfile
+    limit = args.serve_seconds + 300.0
+    with tempfile.TemporaryDirectory(prefix="propag_serve_") as tmp:
+        path = os.path.join(tmp, "master.npz")
+        np.savez(path, **terrain)
+        cmd = [sys.executable, os.path.abspath(__file__), "--serve-only", "--serve-seconds",
+               str(args.serve_seconds), "--serve-rate", str(args.serve_rate), "--serve-terrain", path]
+        try:
+            out = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=None, text=True, timeout=limit)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"the serving run did not finish within {limit:.0f} s"}
+    lines = [x for x in out.stdout.splitlines() if x.startswith("{")]
+    if out.returncode != 0 or not lines:
+        return {"unavailable": f"the serving run failed (exit {out.returncode})"}
+    return json.loads(lines[-1])
 
 
 def bench_b200(args):
@@ -658,8 +703,9 @@ def bench_b200(args):
         del batch
     if args.serve_seconds > 0 and args.workload == "config1":
         _log("serving leg ...")
-        line["serving"] = serve_leg(lib, L, pp, dev, sc.terrain, args.serve_seconds, args.serve_rate,
-                                    150.0)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()  # the child reserves most of the device for its server
+        line["serving"] = serving_child(args, sc.terrain)
     if rank == 0 and not args.no_cpu:
         _log("CPU baseline ...")
         line["cpu_baseline"] = cpu_baseline(sc, stats["evaluations"], os.cpu_count() or 1)
