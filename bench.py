@@ -499,7 +499,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ensemble", type=int, default=256, help="members of the ensemble leg (0 = skip)")
     ap.add_argument("--uneven", type=int, default=64, help="scenarios of the uneven leg (0 = skip)")
-    ap.add_argument("--serve-seconds", type=float, default=90.0,
+    ap.add_argument("--serve-seconds", type=float, default=30.0,
                     help="length of the serving leg's arrival stream (0 = skip)")
     ap.add_argument("--serve-only", action="store_true",
                     help="run the serving leg alone and print its JSON object (the main run "
@@ -532,7 +532,11 @@ def serve_only(args):
             master = {k: z[k] for k in z.files}
     else:
         master = S.config1(size=4096).terrain
-    res = serve_leg(L.lib(), L, pp, dev, master, args.serve_seconds, args.serve_rate, 150.0)
+    # The server reserves its budget up front; the requests' own buffers
+    # (terrain windows, fire rasters, outputs: up to 1 GB each, dozens in
+    # flight) need the rest of the device, so the budget is well below
+    # config 4's 150 GB, which this device could not hold beside them.
+    res = serve_leg(L.lib(), L, pp, dev, master, args.serve_seconds, args.serve_rate, 60.0)
     print(json.dumps(res), flush=True)
 
 
@@ -541,7 +545,7 @@ def serving_child(args, terrain: dict) -> dict:
     server that falls behind its arrivals (config 4's windows reach 4096^2,
     a quarter of them 2048^2 or more) cannot stall the benchmark."""
     import tempfile
-    limit = args.serve_seconds + 300.0
+    limit = args.serve_seconds + 240.0
     with tempfile.TemporaryDirectory(prefix="propag_serve_") as tmp:
         path = os.path.join(tmp, "master.npz")
         np.savez(path, **terrain)
