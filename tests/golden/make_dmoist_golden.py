@@ -6,7 +6,8 @@ reference's own tests parse them (crates/dmoist/src/lib.rs:725-811): lines
 lines are skipped.  The wind files have no test in the reference; their
 "u, v -> value" lines (with or without parentheses) are kept as well.
 
-Run in a checkout where the reference sources exist:
+Run where the reference sources exist ($PROPAG_REFERENCE, else a
+`reference` folder beside this repository):
     python tests/golden/make_dmoist_golden.py
 """
 import os
@@ -15,7 +16,8 @@ import re
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-FIXTURES = "/root/reference/crates/dmoist/fixtures"
+REFERENCE = os.environ.get("PROPAG_REFERENCE") or os.path.join(HERE, "..", "..", "..", "reference")
+FIXTURES = os.path.join(REFERENCE, "crates", "dmoist", "fixtures")
 
 FILES = {
     "hcb": "hcb.txt",
