@@ -447,6 +447,23 @@ int propag_run_host(const Settings *settings, const PropagTerrainPtrs *terrain,
 int64_t propag_rasterize_ignitions(const GeoReference *geo_ref, const FFITimeFeature *features,
                                    uint64_t n_features, PropagIgnition *out, uint64_t max_out);
 
+/* GeoPackage layers as the reference's write_refs / write_boundaries write
+ * them through GDAL (crates/propag/src/propag.rs:601-750), without GDAL:
+ * propag_write_refs_gpkg writes layer "fire_references", one LineString per
+ * burned cell (time < FLT_MAX) from its reference cell's centre to its own,
+ * cells in the reference's order (columns outer); propag_write_boundaries_gpkg
+ * writes layer "grids" (the outlines of the super-grid tiles of side `tile`,
+ * 0 = PROPAG_DEFAULT_TILE) to grid_path and layer "blocks" (their 19 x 19
+ * thread blocks) to block_path; a NULL or empty path skips that layer.  Each
+ * file is a new GeoPackage (an existing one is replaced); the layer's CRS
+ * row keeps the grid's projection string (a GeoPackage wants WKT, which needs
+ * a projection library).  Needs SQLite's runtime library (libsqlite3.so.0).
+ * Host only, no GPU. */
+int propag_write_refs_gpkg(const GeoReference *geo_ref, const float *time, const uint16_t *refs_x,
+                           const uint16_t *refs_y, const char *path);
+int propag_write_boundaries_gpkg(const GeoReference *geo_ref, int32_t tile, const char *grid_path,
+                                 const char *block_path);
+
 /* Writes width*height arrival times as a single-band float32 GeoTIFF, tiled
  * 256 x 256, with the geo transform and nodata f32::MAX, as write_times does
  * (crates/propag/src/propag.rs:576-600). */

@@ -1505,36 +1505,37 @@ extern "C" bool propag_rasterize_fuels(const FFIFuelFeature *fuels, uintptr_t fu
   return true;
 }
 
-// Writes one WKT geometry per line as CSV (GDAL reads it with the CSV driver);
-// stands in for the reference's GPKG layers (propag.rs:601-750).
-static bool write_wkt_csv(const std::string &path, const std::vector<std::string> &rows,
-                          std::string &err) {
-  FILE *f = std::fopen(path.c_str(), "w");
-  if (!f) {
-    err = "cannot open " + path;
-    return false;
-  }
-  std::fputs("WKT\n", f);
-  for (const std::string &r : rows) {
-    std::fputc('"', f);
-    std::fputs(r.c_str(), f);
-    std::fputs("\"\n", f);
-  }
-  return std::fclose(f) == 0;
+namespace propag {  // gpkg.cpp
+bool write_refs_gpkg(const GeoReference &g, const float *time, const uint16_t *rx,
+                     const uint16_t *ry, const std::string &path, std::string &err);
+bool write_boundaries_gpkg(const GeoReference &g, uint32_t tile, uint32_t block,
+                           const std::string &grid_path, const std::string &block_path,
+                           std::string &err);
+}  // namespace propag
+
+// The reference's launch geometry behind its "grids" and "blocks" layers: a
+// super-grid tile of the default side, thread blocks of 19 x 19 cells
+// (crates/propag/src/propag.rs:33,392-418).
+constexpr uint32_t kOutlineBlock = 19;
+
+extern "C" int propag_write_refs_gpkg(const GeoReference *g, const float *time,
+                                      const uint16_t *refs_x, const uint16_t *refs_y,
+                                      const char *path) {
+  if (!g || !time || !refs_x || !refs_y || !path || !*path) return fail(PROPAG_ERR_INVALID, "null argument");
+  std::string err;
+  if (!write_refs_gpkg(*g, time, refs_x, refs_y, path, err)) return fail(PROPAG_ERR_INVALID, err);
+  return PROPAG_OK;
 }
 
-static std::string pt_str(const GeoReference &g, double c, double r) {
-  const GT &t = g.transform.gt;
-  const double x = (double)t.x0 + c * (double)t.dx + r * (double)t.rx;
-  const double y = (double)t.y0 + c * (double)t.ry + r * (double)t.dy;
-  char b[96];
-  std::snprintf(b, sizeof(b), "%.9g %.9g", x, y);
-  return b;
-}
-
-static std::string rect_wkt(const GeoReference &g, double c0, double r0, double c1, double r1) {
-  return "POLYGON((" + pt_str(g, c0, r0) + ", " + pt_str(g, c1, r0) + ", " + pt_str(g, c1, r1) +
-         ", " + pt_str(g, c0, r1) + ", " + pt_str(g, c0, r0) + "))";
+extern "C" int propag_write_boundaries_gpkg(const GeoReference *g, int32_t tile,
+                                            const char *grid_path, const char *block_path) {
+  if (!g) return fail(PROPAG_ERR_INVALID, "null geo_ref");
+  const uint32_t T = tile > 0 ? (uint32_t)tile : PROPAG_DEFAULT_TILE;
+  std::string err;
+  if (!write_boundaries_gpkg(*g, T, kOutlineBlock, grid_path ? grid_path : "",
+                             block_path ? block_path : "", err))
+    return fail(PROPAG_ERR_INVALID, err);
+  return PROPAG_OK;
 }
 
 extern "C" bool FFIPropagation_run(FFIPropagation p, uintptr_t err_len, char *err_msg) {
@@ -1595,44 +1596,21 @@ extern "C" bool FFIPropagation_run(FFIPropagation p, uintptr_t err_len, char *er
       copy_err(err_msg, err_len, err);
       return false;
     }
-    if (p.refs_output_path && *p.refs_output_path) {  // write_refs, propag.rs:699-750
-      std::vector<std::string> rows;
-      for (uint32_t i = 0; i < g.width; ++i)
-        for (uint32_t j = 0; j < g.height; ++j) {
-          const uint64_t ix = i + (uint64_t)j * g.width;
-          if (time[ix] < FLT_MAX)
-            rows.push_back("LINESTRING(" + pt_str(g, rx[ix] + 0.5, ry[ix] + 0.5) + ", " +
-                           pt_str(g, i + 0.5, j + 0.5) + ")");
-        }
-      if (!write_wkt_csv(p.refs_output_path, rows, err)) {
-        copy_err(err_msg, err_len, err);
-        return false;
-      }
+    if (p.refs_output_path && *p.refs_output_path &&  // write_refs, propag.rs:699-750
+        !write_refs_gpkg(g, time.data(), rx.data(), ry.data(), p.refs_output_path, err)) {
+      copy_err(err_msg, err_len, err);
+      return false;
     }
-    // tile outlines (write_boundaries, propag.rs:601-697): the "grid" layer is
-    // the super-grid tile, the "block" layer its 19 x 19 thread blocks
+    // tile outlines (write_boundaries, propag.rs:601-697): the "grids" layer
+    // is the super-grid tiles, the "blocks" layer their 19 x 19 thread blocks
     const bool want_grid = p.grid_boundaries_out_path && *p.grid_boundaries_out_path;
     const bool want_block = p.block_boundaries_out_path && *p.block_boundaries_out_path;
-    if (want_grid || want_block) {
-      const uint32_t T = PROPAG_DEFAULT_TILE, B = 19;
-      const uint32_t sx = (g.width + T - 1) / T, sy = (g.height + T - 1) / T;
-      std::vector<std::string> grids, blocks;
-      for (uint32_t gy = 0; gy < sy; ++gy)
-        for (uint32_t gx = 0; gx < sx; ++gx) {
-          grids.push_back(rect_wkt(g, gx * T, gy * T, (gx + 1) * T, (gy + 1) * T));
-          for (uint32_t by = 0; by < T / B; ++by)
-            for (uint32_t bx = 0; bx < T / B; ++bx)
-              blocks.push_back(rect_wkt(g, gx * T + bx * B, gy * T + by * B, gx * T + (bx + 1) * B,
-                                        gy * T + (by + 1) * B));
-        }
-      if (want_grid && !write_wkt_csv(p.grid_boundaries_out_path, grids, err)) {
-        copy_err(err_msg, err_len, err);
-        return false;
-      }
-      if (want_block && !write_wkt_csv(p.block_boundaries_out_path, blocks, err)) {
-        copy_err(err_msg, err_len, err);
-        return false;
-      }
+    if ((want_grid || want_block) &&
+        !write_boundaries_gpkg(g, PROPAG_DEFAULT_TILE, kOutlineBlock,
+                               want_grid ? p.grid_boundaries_out_path : "",
+                               want_block ? p.block_boundaries_out_path : "", err)) {
+      copy_err(err_msg, err_len, err);
+      return false;
     }
     return true;
   } catch (const std::exception &ex) {  // catch_unwind, propag.rs:280-308

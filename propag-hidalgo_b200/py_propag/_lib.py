@@ -227,6 +227,10 @@ SIGNATURES = {
     "propag_rasterize_ignitions": (C.c_int64, [C.POINTER(GeoReference), C.POINTER(FFITimeFeature),
                                                C.c_uint64, C.POINTER(PropagIgnition), C.c_uint64]),
     "propag_write_geotiff": (C.c_int, [C.POINTER(GeoReference), C.c_void_p, C.c_char_p]),
+    "propag_write_refs_gpkg": (C.c_int, [C.POINTER(GeoReference), C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_char_p]),
+    "propag_write_boundaries_gpkg": (C.c_int, [C.POINTER(GeoReference), C.c_int32, C.c_char_p,
+                                               C.c_char_p]),
 }
 
 _lib = None

@@ -365,3 +365,75 @@ def test_geotiff_round_trip(pp, tmp_path, w, h):
     assert np.array_equal(out, data)
     with pytest.raises(pp.PropagValidationError):
         pp.write_geotiff(path, g, data.ravel()[:10])
+
+
+def _gpkg_geoms(path, layer):
+    """(geometry type name, srs id, [(x, y), ...] per feature) read back with
+    SQLite, decoding the GeoPackage blob header and the little-endian WKB."""
+    import sqlite3
+    import struct
+    db = sqlite3.connect(path)
+    assert db.execute("PRAGMA application_id").fetchone()[0] == 0x47504B47
+    (gtype, srs), = db.execute("SELECT geometry_type_name, srs_id FROM gpkg_geometry_columns "
+                               "WHERE table_name = ?", (layer,)).fetchall()
+    assert db.execute("SELECT data_type FROM gpkg_contents WHERE table_name = ?",
+                      (layer,)).fetchone()[0] == "features"
+    out = []
+    for (blob,) in db.execute(f'SELECT geom FROM "{layer}" ORDER BY fid'):
+        assert blob[:2] == b"GP" and blob[3] == 0x03
+        assert struct.unpack_from("<i", blob, 4)[0] == srs
+        wkb = blob[8 + 32:]
+        order, typ = wkb[0], struct.unpack_from("<I", wkb, 1)[0]
+        assert order == 1
+        o = 5
+        if typ == 3:
+            assert struct.unpack_from("<I", wkb, o)[0] == 1
+            o += 4
+        n = struct.unpack_from("<I", wkb, o)[0]
+        pts = struct.unpack_from(f"<{2 * n}d", wkb, o + 4)
+        out.append(list(zip(pts[0::2], pts[1::2])))
+    db.close()
+    return gtype, srs, out
+
+
+def test_refs_geopackage(lib, pp, tmp_path):
+    """propag_write_refs_gpkg: one LineString per burned cell, from its
+    reference's centre to its own, columns outer (propag.rs:699-750)."""
+    g = _georef(pp, w=4, h=3)
+    time = np.full(12, np.finfo(np.float32).max, np.float32)
+    rx = np.zeros(12, np.uint16)
+    ry = np.zeros(12, np.uint16)
+    burned = [(0, 0, 0, 0), (2, 1, 0, 0), (1, 2, 2, 1)]  # (x, y, ref x, ref y)
+    for (x, y, a, b) in burned:
+        time[x + y * 4] = 10.0
+        rx[x + y * 4], ry[x + y * 4] = a, b
+    path = str(tmp_path / "refs.gpkg")
+    assert lib.propag_write_refs_gpkg(C.byref(g.inner), time.ctypes.data, rx.ctypes.data,
+                                      ry.ctypes.data, path.encode()) == 0
+    gtype, srs, geoms = _gpkg_geoms(path, "fire_references")
+    assert gtype == "LINESTRING"
+    centre = lambda c, r: (1000.0 + (c + 0.5) * 5.0, 2000.0 + (r + 0.5) * 5.0)
+    want = [[centre(a, b), centre(x, y)] for (x, y, a, b) in sorted(burned)]
+    assert geoms == want
+    # a second call replaces the file
+    time[:] = np.finfo(np.float32).max
+    assert lib.propag_write_refs_gpkg(C.byref(g.inner), time.ctypes.data, rx.ctypes.data,
+                                      ry.ctypes.data, path.encode()) == 0
+    assert _gpkg_geoms(path, "fire_references")[2] == []
+
+
+def test_boundaries_geopackage(lib, pp, tmp_path):
+    """propag_write_boundaries_gpkg: the super-grid tiles ("grids") and their
+    19 x 19 thread blocks ("blocks") as closed polygons (propag.rs:601-697)."""
+    g = _georef(pp, w=100, h=80)
+    gp, bp = str(tmp_path / "grids.gpkg"), str(tmp_path / "blocks.gpkg")
+    assert lib.propag_write_boundaries_gpkg(C.byref(g.inner), 57, gp.encode(), bp.encode()) == 0
+    gtype, _, grids = _gpkg_geoms(gp, "grids")
+    assert gtype == "POLYGON" and len(grids) == 2 * 2
+    assert grids[0] == [(1000.0, 2000.0), (1285.0, 2000.0), (1285.0, 2285.0), (1000.0, 2285.0),
+                        (1000.0, 2000.0)]
+    _, _, blocks = _gpkg_geoms(bp, "blocks")
+    assert len(blocks) == 4 * 3 * 3
+    assert blocks[1][0] == (1000.0 + 19 * 5.0, 2000.0)
+    assert lib.propag_write_boundaries_gpkg(C.byref(g.inner), 0, gp.encode(), None) == 0
+    assert len(_gpkg_geoms(gp, "grids")[2]) == 1
