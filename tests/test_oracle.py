@@ -273,3 +273,28 @@ def test_dda_second_cell_is_the_neighbour_in_direction(oracle):
         want = (sx, sy) if abs(x) == abs(y) else ((sx, 0) if abs(x) > abs(y) else (0, sy))
         got = tuple(int(v) for v in oracle.dda_cells(0, 0, x, y)[1])
         assert got == want, (x, y, got, want)
+
+
+def test_arithmetic_moves_the_fixpoint(oracle):
+    """The reference kernel's float operations matter to the last bit: the
+    same scenario in the portable arithmetic (trig 0) and with libm's
+    cosine/arctangent and the reference's fused multiply-adds (trig 2)
+    adopts other references in some cells and moves their times by more
+    than max(0.5 s, 1e-4 t) -- which is why the engine's default arithmetic
+    is the reference's own (oracle/measure_arith.py measures it at full
+    size)."""
+    from py_propag import scenarios as S
+    sc = S.config0(size=256, seed=3)
+    f, _ = oracle.burn_f64(sc.terrain)
+    sp, az, ec = (f[:, k].astype(np.float32) for k in (4, 5, 6))
+    runs = [oracle.propagate(sc.width, sc.height, sc.dx, sc.dy, sc.max_time, sp, az, ec, sc.ignitions,
+                             tile=57, full=2, trig=t) for t in (0, 2)]
+    a, b = (r.time.astype(np.float64) for r in runs)
+    fmax = np.finfo(np.float32).max
+    both = (runs[0].time < fmax) & (runs[1].time < fmax)
+    assert both.sum() > 1000
+    assert (runs[0].time.view(np.uint32) != runs[1].time.view(np.uint32)).any()
+    assert ((runs[0].refs_x != runs[1].refs_x) | (runs[0].refs_y != runs[1].refs_y)).any()
+    dev = np.abs(a - b)[both]
+    assert np.median(dev) < 0.5  # most cells agree closely ...
+    assert (dev > np.maximum(0.5, 1e-4 * a[both])).any()  # ... some do not
