@@ -447,6 +447,37 @@ int propag_run_host(const Settings *settings, const PropagTerrainPtrs *terrain,
 int64_t propag_rasterize_ignitions(const GeoReference *geo_ref, const FFITimeFeature *features,
                                    uint64_t n_features, PropagIgnition *out, uint64_t max_out);
 
+/* Rasterisation on the device.  The host parses the WKB and maps the vertices
+ * to pixel space; the burning runs on the GPU with the same rules as the
+ * host rasteriser above, and the rasters are bit-identical to its result.
+ * All three are stream-ordered on `stream`; the device scratch they need is
+ * allocated and released on that stream (cudaMallocAsync / cudaFreeAsync).
+ *
+ * propag_rasterize_times_device writes the initial time raster of the
+ * reference's rasterize_times (crates/propag/src/propag.rs:837-890):
+ * times[width*height] (device, 4-byte aligned) = the time of the last feature
+ * that burns the cell, FLT_MAX where none does.  Returns without waiting. */
+int propag_rasterize_times_device(const GeoReference *geo_ref, const FFITimeFeature *features,
+                                  uint64_t n_features, float *times, void *stream);
+
+/* The fuel raster of propag_rasterize_fuels (crates/propag/src/propag.rs:
+ * 892-982) into device memory: result[width*height] = the code of the last
+ * feature that burns the cell, 255 (nodata) elsewhere; the same CRS rule.
+ * Holds 4 bytes per cell of device scratch while it runs.  Returns without
+ * waiting. */
+int propag_rasterize_fuels_device(const FFIFuelFeature *fuels, uintptr_t fuels_len,
+                                  const char *fuels_crs, const GeoReference *geo_ref,
+                                  uint8_t *result, void *stream);
+
+/* The ignition list of a device time raster, for PropagJob.ignitions: one
+ * entry per cell whose time is not FLT_MAX, in row-major order.  It starts
+ * the same propagation as propag_rasterize_ignitions' list of the same
+ * features (a list with repeats, where the last entry of a cell wins).
+ * Writes at most max_out entries to out (device; NULL when max_out is 0),
+ * waits for the stream and returns the number of such cells (< 0 on error). */
+int64_t propag_ignitions_from_times_device(const float *times, uint32_t width, uint32_t height,
+                                           PropagIgnition *out, uint64_t max_out, void *stream);
+
 /* GeoPackage layers as the reference's write_refs / write_boundaries write
  * them through GDAL (crates/propag/src/propag.rs:601-750), without GDAL:
  * propag_write_refs_gpkg writes layer "fire_references", one LineString per

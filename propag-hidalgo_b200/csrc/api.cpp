@@ -1505,6 +1505,176 @@ extern "C" bool propag_rasterize_fuels(const FFIFuelFeature *fuels, uintptr_t fu
   return true;
 }
 
+// ========================================== rasterisation on the device ====
+namespace propag {
+cudaError_t launch_rasterize_winner(const RasterPlanDev &p, int64_t W, int64_t H, int32_t *win,
+                                    int sm_count, cudaStream_t stream);
+cudaError_t launch_finish_times(float *times, const float *value, int64_t n, int sm_count,
+                                cudaStream_t stream);
+cudaError_t launch_finish_codes(const int32_t *win, const uint8_t *value, uint8_t *out, int64_t n,
+                                int sm_count, cudaStream_t stream);
+uint64_t burning_chunks(int64_t n);
+cudaError_t launch_burning_list(const float *times, int64_t W, int64_t H, uint32_t *counts,
+                                uint64_t *offsets, PropagIgnition *out, uint64_t max_out,
+                                int sm_count, cudaStream_t stream);
+}  // namespace propag
+
+namespace {
+
+// A stream-ordered device allocation, released on the same stream.
+struct StreamBuf {
+  void *p = nullptr;
+  cudaStream_t s = nullptr;
+  ~StreamBuf() {
+    if (p) cudaFreeAsync(p, s);
+  }
+};
+
+size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// Copies a plan and its features' values (segments | polygons | edges |
+// values, each 16-byte aligned) into one device allocation.
+int upload_plan(const RasterPlan &plan, const void *values, size_t value_bytes, cudaStream_t s,
+                StreamBuf &buf, RasterPlanDev &dev, const void *&dev_values) {
+  const size_t bs = align16(plan.segs.size() * sizeof(RasterSeg));
+  const size_t bp = align16(plan.polys.size() * sizeof(RasterPoly));
+  const size_t be = align16(plan.edges.size() * sizeof(RasterEdge));
+  const size_t total = bs + bp + be + align16(value_bytes);
+  dev = RasterPlanDev{};
+  dev_values = nullptr;
+  buf.s = s;
+  if (total == 0) return PROPAG_OK;
+  std::vector<uint8_t> host(total, 0);
+  if (bs) std::memcpy(host.data(), plan.segs.data(), plan.segs.size() * sizeof(RasterSeg));
+  if (bp) std::memcpy(host.data() + bs, plan.polys.data(), plan.polys.size() * sizeof(RasterPoly));
+  if (be) std::memcpy(host.data() + bs + bp, plan.edges.data(), plan.edges.size() * sizeof(RasterEdge));
+  if (value_bytes) std::memcpy(host.data() + bs + bp + be, values, value_bytes);
+  CK(cudaMallocAsync(&buf.p, total, s));
+  // from pageable memory: returns once the bytes are staged, so `host` may go
+  CK(cudaMemcpyAsync(buf.p, host.data(), total, cudaMemcpyHostToDevice, s));
+  char *d = static_cast<char *>(buf.p);
+  dev.segs = reinterpret_cast<const RasterSeg *>(d);
+  dev.nseg = plan.segs.size();
+  dev.samples = plan.samples;
+  dev.polys = reinterpret_cast<const RasterPoly *>(d + bs);
+  dev.npoly = plan.polys.size();
+  dev.rows = plan.rows;
+  dev.edges = reinterpret_cast<const RasterEdge *>(d + bs + bp);
+  dev_values = d + bs + bp + be;
+  return PROPAG_OK;
+}
+
+// Parses features i (skipping missing and invalid WKB, as the host
+// rasterisers do) into a plan, feature index = position in the input.
+template <typename GetWkb>
+RasterPlan plan_features(const GeoReference &g, uint64_t n, GetWkb &&wkb) {
+  RasterPlan plan;
+  for (uint64_t i = 0; i < n; ++i) {
+    const uint8_t *data = nullptr;
+    uintptr_t len = 0;
+    wkb(i, data, len);
+    if (!data || len == 0) continue;
+    Geometry geom;
+    if (!parse_wkb(data, len, geom)) continue;
+    plan_geometry(g, geom, (int32_t)i, plan);
+  }
+  return plan;
+}
+
+}  // namespace
+
+extern "C" int propag_rasterize_times_device(const GeoReference *g, const FFITimeFeature *f,
+                                             uint64_t n, float *times, void *stream) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (!g || !times) return fail(PROPAG_ERR_INVALID, "null geo_ref or times");
+  if (n && !f) return fail(PROPAG_ERR_INVALID, "null features");
+  if (!valid_size(g->width, g->height)) return fail(PROPAG_ERR_INVALID, "width/height must be 1..65534");
+  if (n > 0x7FFFFFFFull) return fail(PROPAG_ERR_INVALID, "too many features");
+  if ((uintptr_t)times % alignof(float)) return fail(PROPAG_ERR_INVALID, "times is not 4-byte aligned");
+  const cudaStream_t s = (cudaStream_t)stream;
+  const RasterPlan plan = plan_features(*g, n, [&](uint64_t i, const uint8_t *&d, uintptr_t &l) {
+    d = f[i].geom_wkb;
+    l = f[i].geom_wkb_len;
+  });
+  std::vector<float> value(n);
+  for (uint64_t i = 0; i < n; ++i) value[i] = f[i].time;
+  StreamBuf buf;
+  RasterPlanDev dev;
+  const void *dev_value;
+  rc = upload_plan(plan, value.data(), n * sizeof(float), s, buf, dev, dev_value);
+  if (rc) return rc;
+  const int64_t W = g->width, H = g->height;
+  CK(launch_rasterize_winner(dev, W, H, reinterpret_cast<int32_t *>(times), sms, s));
+  CK(launch_finish_times(times, static_cast<const float *>(dev_value), W * H, sms, s));
+  return PROPAG_OK;
+}
+
+extern "C" int propag_rasterize_fuels_device(const FFIFuelFeature *fuels, uintptr_t n,
+                                             const char *fuels_crs, const GeoReference *g,
+                                             uint8_t *result, void *stream) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (!g || !result) return fail(PROPAG_ERR_INVALID, "null geo_ref or result");
+  if (n && !fuels) return fail(PROPAG_ERR_INVALID, "null features");
+  if (!fuels_crs) return fail(PROPAG_ERR_INVALID, "invalid fuels CRS");
+  if (!valid_size(g->width, g->height)) return fail(PROPAG_ERR_INVALID, "width/height must be 1..65534");
+  if (n > 0x7FFFFFFFull) return fail(PROPAG_ERR_INVALID, "too many features");
+  const std::string grid = norm_crs((const char *)g->proj), src = norm_crs(fuels_crs);
+  if (!src.empty() && src != grid)
+    return fail(PROPAG_ERR_INVALID,
+                "fuels CRS differs from the grid CRS; this build does not reproject (pass geometries in the grid CRS)");
+  const cudaStream_t s = (cudaStream_t)stream;
+  const RasterPlan plan = plan_features(*g, n, [&](uint64_t i, const uint8_t *&d, uintptr_t &l) {
+    d = fuels[i].geom_wkb;
+    l = fuels[i].geom_wkb_len;
+  });
+  std::vector<uint8_t> value(n);
+  for (uint64_t i = 0; i < n; ++i) value[i] = fuels[i].code;
+  StreamBuf buf, win;
+  RasterPlanDev dev;
+  const void *dev_value;
+  rc = upload_plan(plan, value.data(), n, s, buf, dev, dev_value);
+  if (rc) return rc;
+  const int64_t W = g->width, H = g->height;
+  win.s = s;
+  CK(cudaMallocAsync(&win.p, (size_t)(W * H) * sizeof(int32_t), s));
+  int32_t *w = static_cast<int32_t *>(win.p);
+  CK(launch_rasterize_winner(dev, W, H, w, sms, s));
+  CK(launch_finish_codes(w, static_cast<const uint8_t *>(dev_value), result, W * H, sms, s));
+  return PROPAG_OK;
+}
+
+extern "C" int64_t propag_ignitions_from_times_device(const float *times, uint32_t width,
+                                                      uint32_t height, PropagIgnition *out,
+                                                      uint64_t max_out, void *stream) {
+  int sms = 0;
+  int rc = ensure_device(-1, &sms);
+  if (rc) return rc;
+  if (!times) return fail(PROPAG_ERR_INVALID, "null times");
+  if (max_out && !out) return fail(PROPAG_ERR_INVALID, "null out with max_out > 0");
+  if (!valid_size(width, height)) return fail(PROPAG_ERR_INVALID, "width/height must be 1..65534");
+  if ((uintptr_t)times % alignof(float) || (uintptr_t)out % alignof(PropagIgnition))
+    return fail(PROPAG_ERR_INVALID, "times or out is not 4-byte aligned");
+  const cudaStream_t s = (cudaStream_t)stream;
+  const int64_t W = width, H = height;
+  const uint64_t chunks = burning_chunks(W * H);
+  const size_t bc = align16(chunks * sizeof(uint32_t));
+  StreamBuf buf;
+  buf.s = s;
+  CK(cudaMallocAsync(&buf.p, bc + (chunks + 1) * sizeof(uint64_t), s));
+  uint32_t *counts = static_cast<uint32_t *>(buf.p);
+  uint64_t *offsets = reinterpret_cast<uint64_t *>(static_cast<char *>(buf.p) + bc);
+  CK(launch_burning_list(times, W, H, counts, offsets, out, max_out, sms, s));
+  uint64_t total = 0;
+  // into pageable memory: returns when the copy (and the work ahead of it) is done
+  CK(cudaMemcpyAsync(&total, offsets + chunks, sizeof(total), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return (int64_t)total;
+}
+
 namespace propag {  // gpkg.cpp
 bool write_refs_gpkg(const GeoReference &g, const float *time, const uint16_t *rx,
                      const uint16_t *ry, const std::string &path, std::string &err);

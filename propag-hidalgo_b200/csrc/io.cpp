@@ -122,6 +122,32 @@ bool parse_wkb(const uint8_t *data, size_t len, Geometry &out) {
   return true;
 }
 
+void plan_geometry(const GeoReference &g, const Geometry &geom, int32_t feature, RasterPlan &plan) {
+  const int64_t W = g.width, H = g.height;
+  for (const Pt &p : geom.points) {
+    double c, r;
+    geo_to_pixel(g, p.x, p.y, c, r);
+    plan_segment(plan, c, r, c, r, feature, W, H);
+  }
+  for (const auto &line : geom.lines)
+    for (size_t k = 0; k + 1 < line.size(); ++k) {
+      double c0, r0, c1, r1;
+      geo_to_pixel(g, line[k].x, line[k].y, c0, r0);
+      geo_to_pixel(g, line[k + 1].x, line[k + 1].y, c1, r1);
+      plan_segment(plan, c0, r0, c1, r1, feature, W, H);
+    }
+  std::vector<std::vector<Pt>> rings;
+  for (const auto &poly : geom.polygons) {
+    rings.assign(poly.size(), {});
+    for (size_t i = 0; i < poly.size(); ++i) {
+      rings[i].resize(poly[i].size());
+      for (size_t k = 0; k < poly[i].size(); ++k)
+        geo_to_pixel(g, poly[i][k].x, poly[i][k].y, rings[i][k].x, rings[i][k].y);
+    }
+    plan_polygon(plan, rings, feature, H);
+  }
+}
+
 bool write_geotiff_f32(const std::string &path, const GeoReference &g, const float *data,
                        std::string &err) {
   const uint32_t W = g.width, H = g.height, T = 256;

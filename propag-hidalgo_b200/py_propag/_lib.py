@@ -226,6 +226,12 @@ SIGNATURES = {
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PropagStats)]),
     "propag_rasterize_ignitions": (C.c_int64, [C.POINTER(GeoReference), C.POINTER(FFITimeFeature),
                                                C.c_uint64, C.POINTER(PropagIgnition), C.c_uint64]),
+    "propag_rasterize_times_device": (C.c_int, [C.POINTER(GeoReference), C.POINTER(FFITimeFeature),
+                                                C.c_uint64, C.c_void_p, C.c_void_p]),
+    "propag_rasterize_fuels_device": (C.c_int, [C.POINTER(FFIFuelFeature), C.c_size_t, C.c_char_p,
+                                                C.POINTER(GeoReference), C.c_void_p, C.c_void_p]),
+    "propag_ignitions_from_times_device": (C.c_int64, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                                       C.c_uint64, C.c_void_p]),
     "propag_write_geotiff": (C.c_int, [C.POINTER(GeoReference), C.c_void_p, C.c_char_p]),
     "propag_write_refs_gpkg": (C.c_int, [C.POINTER(GeoReference), C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_char_p]),
