@@ -682,7 +682,11 @@ def bench_b200(args):
         "roofline": {"bound": "hbm", "kernel": "engine_kernel (propagation)", "achieved": ach,
                      "peak": peak, "unit": "GB/s", "frac": ach / peak,
                      "traffic": DRAM_TRAFFIC.get(args.workload, {}).get("engine_kernel"),
-                     "algorithmic_bytes": prop_bytes, "peak_source": peak_kind},
+                     "algorithmic_bytes": prop_bytes, "peak_source": peak_kind,
+                     "cell_updates_per_s": stats["evaluations"] / prop_s,
+                     "sweeps": stats["sweeps"],
+                     "bytes_per_sweep": prop_bytes / max(1, stats["sweeps"]),
+                     "full_grid_bytes_per_sweep": 20 * N},
         "kernels": {"fire_kernel": {"achieved": fire_ach, "peak": peak, "unit": "GB/s",
                                     "frac": fire_ach / peak, "bytes": FIRE_BYTES_PER_CELL * N,
                                     "traffic": DRAM_TRAFFIC.get(args.workload, {}).get("fire_kernel")}},
