@@ -10,6 +10,12 @@
  * and converts the imperial outputs to the same 10 SI fields as the FP64
  * restatement in oracle/firelib_oracle.c.  Fuel codes outside 1..13 produce
  * zeros (the Rust catalog has no fire for them).
+ *
+ * ref_burn_c_rust_catalog does the same with one entry of the C catalog set
+ * to the Rust catalog's value: the 10-h dead load of NFFL13, 1.0580 in
+ * fireLib.c (fireLib.c:1316) and 0.0580 in crates/firelib/src/lib.rs:262.
+ * The reference's own quickcheck comparison draws fuel codes 0..12 only
+ * (lib.rs:417), so it never meets that difference.
  */
 #include "fireLib.h"
 #include <stdint.h>
@@ -17,12 +23,19 @@
 static const double FOOT_TO_M = 0.3048;
 static const double BTU = 1054.35;
 
-int64_t ref_burn_c(int64_t n, const uint8_t *fuel, const float *d1, const float *d10,
-                   const float *d100, const float *herb, const float *wood,
-                   const float *wind_speed, const float *wind_azimuth, const float *slope,
-                   const float *aspect, double *out) {
+static int64_t burn(int rust_nffl13, int64_t n, const uint8_t *fuel, const float *d1,
+                    const float *d10, const float *d100, const float *herb, const float *wood,
+                    const float *wind_speed, const float *wind_azimuth, const float *slope,
+                    const float *aspect, double *out) {
   FuelCatalogPtr cat = Fire_FuelCatalogCreateStandard("standard", 13);
   if (!cat) return -1;
+  /* particle 1 of model 13 is its 10-h dead class; its surface area is set
+     from the load when the particle is added (fireLib.c:1719), the
+     combustion terms on the model's first spread call */
+  if (rust_nffl13) {
+    Fuel_Load(cat, 13, 1) = 0.0580;
+    Fuel_SurfaceArea(cat, 13, 1) = Fuel_Load(cat, 13, 1) * Fuel_Savr(cat, 13, 1) / Fuel_Density(cat, 13, 1);
+  }
   int64_t burning = 0;
   for (int64_t i = 0; i < n; i++) {
     double *o = out + i * 10;
@@ -50,4 +63,18 @@ int64_t ref_burn_c(int64_t n, const uint8_t *fuel, const float *d1, const float 
   }
   Fire_FuelCatalogDestroy(cat);
   return burning;
+}
+
+int64_t ref_burn_c(int64_t n, const uint8_t *fuel, const float *d1, const float *d10,
+                   const float *d100, const float *herb, const float *wood,
+                   const float *wind_speed, const float *wind_azimuth, const float *slope,
+                   const float *aspect, double *out) {
+  return burn(0, n, fuel, d1, d10, d100, herb, wood, wind_speed, wind_azimuth, slope, aspect, out);
+}
+
+int64_t ref_burn_c_rust_catalog(int64_t n, const uint8_t *fuel, const float *d1, const float *d10,
+                                const float *d100, const float *herb, const float *wood,
+                                const float *wind_speed, const float *wind_azimuth,
+                                const float *slope, const float *aspect, double *out) {
+  return burn(1, n, fuel, d1, d10, d100, herb, wood, wind_speed, wind_azimuth, slope, aspect, out);
 }

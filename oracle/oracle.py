@@ -71,6 +71,7 @@ def _load_ref():
     if _ref is None:
         _ref = C.CDLL(os.path.join(HERE, "_ref", "libfirelib_ref.so"))
         _ref.ref_burn_c.restype = C.c_int64
+        _ref.ref_burn_c_rust_catalog.restype = C.c_int64
     return _ref
 
 
@@ -101,11 +102,15 @@ def burn_f64(terrain: dict) -> tuple[np.ndarray, np.ndarray]:
     return out, sit
 
 
-def burn_firelib_c(terrain: dict) -> np.ndarray:
+def burn_firelib_c(terrain: dict, rust_nffl13: bool = False) -> np.ndarray:
+    """The reference's fireLib.c on each cell (10 SI fields).  rust_nffl13:
+    with NFFL13's 10-h dead load set to the Rust catalog's 0.0580 instead of
+    fireLib.c's 1.0580 (the one entry where the two catalogs differ)."""
     lib = _load_ref()
     n, fuel, rest = _terrain_args(terrain)
     out = np.zeros((n, 10), dtype=np.float64)
-    lib.ref_burn_c(C.c_int64(n), _ptr(fuel), *[_ptr(r) for r in rest], _ptr(out))
+    fn = lib.ref_burn_c_rust_catalog if rust_nffl13 else lib.ref_burn_c
+    fn(C.c_int64(n), _ptr(fuel), *[_ptr(r) for r in rest], _ptr(out))
     return out
 
 

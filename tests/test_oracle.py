@@ -89,6 +89,32 @@ def test_nffl13_follows_the_rust_catalog(oracle):
     assert cat[13, 0] > 0
 
 
+@pytest.mark.parametrize("quickcheck", [True, False])
+def test_live_firelib_c_with_the_rust_nffl13_load(oracle, quickcheck):
+    """With NFFL13's 10-h dead load set to the Rust catalog's value inside
+    fireLib.c (its surface area follows), the FP64 restatement equals the
+    reference's C fireLib on every fuel code, NFFL13 included, to ~1e-13 in
+    every field: that one catalog entry is the whole difference."""
+    if not oracle.have_firelib_c():
+        pytest.skip("reference fireLib.c not built here")
+    t = random_terrain(20_000, 9, quickcheck=quickcheck)
+    t["fuel_code"][::3] = 13
+    ours, _ = oracle.burn_f64(t)
+    c = oracle.burn_firelib_c(t, rust_nffl13=True)
+    for k, name in enumerate(FIELDS):
+        a, b = ours[:, k], c[:, k]
+        if name == "azimuth_max":
+            d = np.abs(np.angle(np.exp(1j * (a - b))))
+            assert np.max(d[c[:, 4] >= 0.00508], initial=0) < 1e-6, name
+        else:
+            err = np.where(np.abs(b) > 1e-9, np.abs(a - b) / np.maximum(np.abs(b), 1e-12), np.abs(a - b))
+            assert np.max(err) < 1e-12, name
+    plain = oracle.burn_firelib_c(t)
+    is13 = t["fuel_code"] == 13
+    moved = np.any(np.abs(plain - c) > 1e-9 * np.maximum(np.abs(c), 1.0), axis=1)
+    assert np.array_equal(moved & ~is13, np.zeros_like(moved)) and moved[is13].mean() > 0.5
+
+
 def test_no_fire_codes(oracle):
     t = random_terrain(64, 8)
     t["fuel_code"][:] = np.array([0, 14, 19, 20, 255, 1, 13, 7], np.uint8)[np.arange(64) % 8]
