@@ -71,7 +71,8 @@ def _load_ref():
     if _ref is None:
         _ref = C.CDLL(os.path.join(HERE, "_ref", "libfirelib_ref.so"))
         _ref.ref_burn_c.restype = C.c_int64
-        _ref.ref_burn_c_rust_catalog.restype = C.c_int64
+        if hasattr(_ref, "ref_burn_c_rust_catalog"):  # absent from builds of older harnesses
+            _ref.ref_burn_c_rust_catalog.restype = C.c_int64
     return _ref
 
 
