@@ -398,3 +398,16 @@ def test_burning_list_logic(n, density):
     total, order = burning_list_as_kernel(t)
     expect = np.flatnonzero(t != np.finfo(np.float32).max)
     assert total == expect.size and order == list(expect)
+
+
+def test_device_rasterisers_need_a_device(L):
+    """Without a GPU the device entry points report PROPAG_ERR_NO_DEVICE
+    (the host rasterisers above keep working)."""
+    import py_propag
+    if py_propag.check_cuda_available():
+        pytest.skip("a GPU is present")
+    lib = L.lib()
+    g = georef(L, 8, 8, GRIDS[0][2])
+    assert lib.propag_rasterize_times_device(C.byref(g), None, 0, None, None) == L.PROPAG_ERR_NO_DEVICE
+    assert lib.propag_rasterize_fuels_device(None, 0, b"", C.byref(g), None, None) == L.PROPAG_ERR_NO_DEVICE
+    assert lib.propag_ignitions_from_times_device(None, 8, 8, None, 0, None) == L.PROPAG_ERR_NO_DEVICE
