@@ -15,7 +15,8 @@
    ballots and carries -> inclusive prefix XOR) against a cumulative XOR,
    the binary search over `before` against searchsorted, and the ignition
    list's count / scan / ballot-compaction against np.flatnonzero.
-The device kernels themselves are compared with the host rasteriser in
+The kernels' own source runs on the CPU against the host rasteriser in
+tests/test_raster_kernels_emulated.py, and on the device in
 tests/test_zz_raster_device.py."""
 import ctypes as C
 import math
