@@ -486,9 +486,12 @@ int64_t propag_ignitions_from_times_device(const float *times, uint32_t width, u
  * writes layer "grids" (the outlines of the super-grid tiles of side `tile`,
  * 0 = PROPAG_DEFAULT_TILE) to grid_path and layer "blocks" (their 19 x 19
  * thread blocks) to block_path; a NULL or empty path skips that layer.  Each
- * file is a new GeoPackage (an existing one is replaced); the layer's CRS
- * row keeps the grid's projection string (a GeoPackage wants WKT, which needs
- * a projection library).  Needs SQLite's runtime library (libsqlite3.so.0).
+ * file is a new GeoPackage (an existing one is replaced).  The layer's CRS
+ * row holds WKT where it needs no projection library or EPSG database
+ * (EPSG:4326, EPSG:326zz / 327zz / 25828-25838, PROJ strings of UTM or
+ * longlat on WGS 84 / GRS 1980), "undefined" otherwise, and the grid's
+ * projection string in its description.  Needs SQLite's runtime library
+ * (libsqlite3.so.0).
  * Host only, no GPU. */
 int propag_write_refs_gpkg(const GeoReference *geo_ref, const float *time, const uint16_t *refs_x,
                            const uint16_t *refs_y, const char *path);

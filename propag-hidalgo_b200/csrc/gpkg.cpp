@@ -10,11 +10,16 @@
 // a GeoPackage binary header followed by the geometry in WKB.  SQLite is
 // used through its C API from the system's runtime library
 // (libsqlite3.so.0), loaded on first use; no GDAL.  The layer's CRS is the
-// grid's projection string, which a GeoPackage wants as WKT: the srs row
-// keeps it in its description, with the definition "undefined".
+// grid's projection string, which a GeoPackage wants as WKT: without a
+// projection library the WKT is written for the CRSs whose definition needs
+// no database (EPSG:4326, WGS 84 and ETRS89 UTM zones by EPSG code, PROJ
+// strings of UTM or longitude/latitude on the WGS 84 or GRS 1980
+// ellipsoid), and "undefined" for others; the srs row's description keeps
+// the projection string either way.
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <cctype>
 #include <cfloat>
 #include <cstdint>
 #include <cstdio>
@@ -118,7 +123,127 @@ std::string sql_quote(const std::string &s) {
   return o + "'";
 }
 
-constexpr int32_t kLayerSrs = 100000;  // the grid's CRS (custom id)
+constexpr int32_t kCustomSrs = 100000;  // srs_id of a CRS without an EPSG code
+
+// One row of gpkg_spatial_ref_sys for the grid's CRS.
+struct SrsRow {
+  int32_t id = kCustomSrs;
+  std::string name = "grid", org = "NONE";
+  int32_t org_id = kCustomSrs;
+  std::string definition = "undefined", description;
+};
+
+// WKT 1 pieces (OGC 01-009) with the EPSG registry's names and constants.
+const char *kWgs84Spheroid = "SPHEROID[\"WGS 84\",6378137,298.257223563,AUTHORITY[\"EPSG\",\"7030\"]]";
+const char *kGrs80Spheroid = "SPHEROID[\"GRS 1980\",6378137,298.257222101,AUTHORITY[\"EPSG\",\"7019\"]]";
+const char *kGreenwichDegree =
+    "PRIMEM[\"Greenwich\",0,AUTHORITY[\"EPSG\",\"8901\"]],"
+    "UNIT[\"degree\",0.0174532925199433,AUTHORITY[\"EPSG\",\"9122\"]]";
+
+std::string wgs84_geogcs() {
+  return std::string("GEOGCS[\"WGS 84\",DATUM[\"WGS_1984\",") + kWgs84Spheroid +
+         ",AUTHORITY[\"EPSG\",\"6326\"]]," + kGreenwichDegree + ",AUTHORITY[\"EPSG\",\"4326\"]]";
+}
+std::string etrs89_geogcs() {
+  return std::string("GEOGCS[\"ETRS89\",DATUM[\"European_Terrestrial_Reference_System_1989\",") +
+         kGrs80Spheroid + ",TOWGS84[0,0,0,0,0,0,0],AUTHORITY[\"EPSG\",\"6258\"]]," + kGreenwichDegree +
+         ",AUTHORITY[\"EPSG\",\"4258\"]]";
+}
+std::string unknown_geogcs(bool grs80) {
+  return std::string("GEOGCS[\"unknown\",DATUM[\"Unknown based on ") + (grs80 ? "GRS 1980" : "WGS 84") +
+         " ellipsoid\"," + (grs80 ? kGrs80Spheroid : kWgs84Spheroid) + "]," + kGreenwichDegree + "]";
+}
+// Universal Transverse Mercator zone 1-60 on `geogcs`; epsg = 0: no authority.
+std::string utm_projcs(const std::string &name, const std::string &geogcs, int zone, bool south, int epsg) {
+  std::string w = "PROJCS[\"" + name + "\"," + geogcs +
+                  ",PROJECTION[\"Transverse_Mercator\"],PARAMETER[\"latitude_of_origin\",0],"
+                  "PARAMETER[\"central_meridian\"," + std::to_string(6 * zone - 183) +
+                  "],PARAMETER[\"scale_factor\",0.9996],PARAMETER[\"false_easting\",500000],"
+                  "PARAMETER[\"false_northing\"," + (south ? "10000000" : "0") +
+                  "],UNIT[\"metre\",1,AUTHORITY[\"EPSG\",\"9001\"]],AXIS[\"Easting\",EAST],"
+                  "AXIS[\"Northing\",NORTH]";
+  if (epsg) w += ",AUTHORITY[\"EPSG\",\"" + std::to_string(epsg) + "\"]";
+  return w + "]";
+}
+
+bool parse_int(const std::string &s, int &v) {
+  if (s.empty() || s.size() > 9) return false;
+  v = 0;
+  for (char c : s) {
+    if (c < '0' || c > '9') return false;
+    v = 10 * v + (c - '0');
+  }
+  return true;
+}
+
+SrsRow srs_row(const std::string &crs) {
+  SrsRow r;
+  r.description = crs;
+  std::vector<std::string> tok;  // whitespace-separated words
+  for (size_t i = 0; i < crs.size();) {
+    while (i < crs.size() && std::isspace((unsigned char)crs[i])) ++i;
+    size_t j = i;
+    while (j < crs.size() && !std::isspace((unsigned char)crs[j])) ++j;
+    if (j > i) tok.push_back(crs.substr(i, j - i));
+    i = j;
+  }
+  auto lower = [](std::string t) {
+    for (char &c : t) c = (char)std::tolower((unsigned char)c);
+    return t;
+  };
+  int code = 0;
+  if (tok.size() == 1 && lower(tok[0]).rfind("epsg:", 0) == 0 && parse_int(tok[0].substr(5), code)) {
+    std::string def;
+    if (code == 4326) def = wgs84_geogcs();
+    else if ((code > 32600 && code <= 32660) || (code > 32700 && code <= 32760))
+      def = utm_projcs("WGS 84 / UTM zone " + std::to_string(code % 100) + (code > 32700 ? "S" : "N"),
+                       wgs84_geogcs(), code % 100, code > 32700, code);
+    else if (code >= 25828 && code <= 25838)
+      def = utm_projcs("ETRS89 / UTM zone " + std::to_string(code % 100) + "N", etrs89_geogcs(),
+                       code % 100, false, code);
+    if (def.empty()) return r;
+    const size_t q = def.find('"') + 1;
+    r.id = r.org_id = code;
+    r.org = "EPSG";
+    r.name = def.substr(q, def.find('"', q) - q);
+    r.definition = def;
+    return r;
+  }
+  // a PROJ string: +proj=utm|longlat|latlong, +zone, +south, +ellps / +datum,
+  // +units=m; anything else leaves the CRS undefined
+  std::string proj, ellps;
+  int zone = 0;
+  bool south = false;
+  for (const std::string &t : tok) {
+    if (t.size() < 2 || t[0] != '+') return r;
+    const size_t eq = t.find('=');
+    const std::string key = t.substr(1, eq == std::string::npos ? std::string::npos : eq - 1);
+    const std::string val = eq == std::string::npos ? "" : t.substr(eq + 1);
+    if (key == "proj") proj = val;
+    else if (key == "zone") {
+      if (!parse_int(val, zone)) return r;
+    } else if (key == "south" && val.empty()) south = true;
+    else if (key == "ellps" || key == "datum") {
+      if (val != "WGS84" && val != "GRS80") return r;
+      if (!ellps.empty() && ellps != val) return r;
+      ellps = val;
+    } else if (key == "units") {
+      if (val != "m") return r;
+    } else if (key == "towgs84") {
+      if (val != "0,0,0" && val != "0,0,0,0,0,0,0") return r;
+    } else if (key != "no_defs" && !(key == "type" && val == "crs")) {
+      return r;
+    }
+  }
+  if (ellps.empty()) return r;
+  const bool grs80 = ellps == "GRS80";
+  if (proj == "utm" && zone >= 1 && zone <= 60)
+    r.definition = utm_projcs("unknown", grs80 ? unknown_geogcs(true) : wgs84_geogcs(), zone, south, 0);
+  else if ((proj == "longlat" || proj == "latlong") && zone == 0 && !south)
+    r.definition = grs80 ? unknown_geogcs(true) : wgs84_geogcs();
+  if (r.definition != "undefined") r.name = "unknown";
+  return r;
+}
 
 // Writes one layer (a new file at `path`) with one feature per geometry
 // (flat x, y pairs); geom_type "LINESTRING" or "POLYGON".
@@ -144,6 +269,7 @@ bool write_layer(const std::string &path, const char *layer, bool polygon,
     return true;
   };
   const std::string t = layer, gt = polygon ? "POLYGON" : "LINESTRING";
+  const SrsRow srs = srs_row(crs);
   double ext[4] = {DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX};
   bool ok =
       exec("PRAGMA application_id = 1196444487; PRAGMA user_version = 10200; BEGIN;") &&
@@ -159,8 +285,11 @@ bool write_layer(const std::string &path, const char *layer, bool polygon,
            "AUTHORITY[\"EPSG\",\"6326\"]],PRIMEM[\"Greenwich\",0,AUTHORITY[\"EPSG\",\"8901\"]],"
            "UNIT[\"degree\",0.0174532925199433,AUTHORITY[\"EPSG\",\"9122\"]],"
            "AUTHORITY[\"EPSG\",\"4326\"]]', 'longitude/latitude coordinates in decimal degrees "
-           "on the WGS 84 spheroid'), ('grid', " + std::to_string(kLayerSrs) + ", 'NONE', " +
-           std::to_string(kLayerSrs) + ", 'undefined', " + sql_quote(crs) + ");") &&
+           "on the WGS 84 spheroid');") &&
+      (srs.id == 4326 ||
+       exec("INSERT INTO gpkg_spatial_ref_sys VALUES (" + sql_quote(srs.name) + ", " +
+            std::to_string(srs.id) + ", " + sql_quote(srs.org) + ", " + std::to_string(srs.org_id) + ", " +
+            sql_quote(srs.definition) + ", " + sql_quote(srs.description) + ");")) &&
       exec("CREATE TABLE gpkg_contents (table_name TEXT NOT NULL PRIMARY KEY, data_type TEXT NOT "
            "NULL, identifier TEXT UNIQUE, description TEXT DEFAULT '', last_change DATETIME NOT "
            "NULL DEFAULT (strftime('%Y-%m-%dT%H:%M:%fZ','now')), min_x DOUBLE, min_y DOUBLE, "
@@ -179,7 +308,7 @@ bool write_layer(const std::string &path, const char *layer, bool polygon,
     ok = s->prepare_v2(db, ins.c_str(), -1, &st, nullptr) == kSqliteOk;
     for (size_t i = 0; ok && i < geoms.size(); ++i) {
       double env[4];
-      const std::vector<uint8_t> blob = gpkg_blob(kLayerSrs, polygon, geoms[i], env);
+      const std::vector<uint8_t> blob = gpkg_blob(srs.id, polygon, geoms[i], env);
       ext[0] = std::min(ext[0], env[0]);
       ext[1] = std::max(ext[1], env[1]);
       ext[2] = std::min(ext[2], env[2]);
@@ -196,9 +325,9 @@ bool write_layer(const std::string &path, const char *layer, bool polygon,
     std::snprintf(b, sizeof(b), "%.17g, %.17g, %.17g, %.17g", ext[0], ext[2], ext[1], ext[3]);
     ok = exec("INSERT INTO gpkg_contents (table_name, data_type, identifier, min_x, min_y, max_x, "
               "max_y, srs_id) VALUES (" + sql_quote(t) + ", 'features', " + sql_quote(t) + ", " + b +
-              ", " + std::to_string(kLayerSrs) + ");") &&
+              ", " + std::to_string(srs.id) + ");") &&
          exec("INSERT INTO gpkg_geometry_columns VALUES (" + sql_quote(t) + ", 'geom', '" + gt +
-              "', " + std::to_string(kLayerSrs) + ", 0, 0);") &&
+              "', " + std::to_string(srs.id) + ", 0, 0);") &&
          exec("COMMIT;");
   }
   s->close(db);

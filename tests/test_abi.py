@@ -422,6 +422,60 @@ def test_refs_geopackage(lib, pp, tmp_path):
     assert _gpkg_geoms(path, "fire_references")[2] == []
 
 
+def _wkt_balanced(w):
+    depth = 0
+    for ch in w:
+        depth += {"[": 1, "]": -1}.get(ch, 0)
+        if depth < 0:
+            return False
+    return depth == 0 and w.count('"') % 2 == 0
+
+
+@pytest.mark.parametrize("crs,srs_id,org,has", [
+    (PROJ, 100000, "NONE", ['PROJCS["unknown"', 'SPHEROID["GRS 1980",6378137,298.257222101',
+                            'PARAMETER["central_meridian",-3]', 'PARAMETER["false_northing",0]']),
+    ("+proj=utm +zone=33 +south +datum=WGS84 +units=m +no_defs", 100000, "NONE",
+     ['GEOGCS["WGS 84"', 'PARAMETER["central_meridian",15]', 'PARAMETER["false_northing",10000000]']),
+    ("EPSG:25830", 25830, "EPSG", ['PROJCS["ETRS89 / UTM zone 30N"', 'AUTHORITY["EPSG","4258"]',
+                                  'AUTHORITY["EPSG","25830"]']),
+    ("epsg:32733", 32733, "EPSG", ['PROJCS["WGS 84 / UTM zone 33S"', 'PARAMETER["false_northing",10000000]']),
+    ("EPSG:4326", 4326, "EPSG", ['GEOGCS["WGS 84"']),
+    ("+proj=longlat +ellps=GRS80 +no_defs", 100000, "NONE", ['GEOGCS["unknown"', 'GRS 1980']),
+    ("+proj=lcc +lat_1=40 +ellps=GRS80", 100000, "NONE", None),  # needs a projection library
+    ("EPSG:2062", 100000, "NONE", None),                         # needs the EPSG database
+])
+def test_geopackage_crs_rows(lib, pp, tmp_path, crs, srs_id, org, has):
+    """The layer's srs row: WKT for the CRSs that need no database (EPSG:4326,
+    WGS 84 and ETRS89 UTM zones, PROJ strings of UTM / longlat on WGS 84 or
+    GRS 1980), "undefined" otherwise; the projection string stays in the
+    description, and the layer and its geometries carry the row's id."""
+    import sqlite3
+    g = pp.PyGeoReference(4, 3, crs, [1000.0, 5.0, 0.0, 2000.0, 0.0, 5.0])
+    time = np.full(12, 1.0, np.float32)
+    zeros = np.zeros(12, np.uint16)
+    path = str(tmp_path / "refs.gpkg")
+    assert lib.propag_write_refs_gpkg(C.byref(g.inner), time.ctypes.data, zeros.ctypes.data,
+                                      zeros.ctypes.data, path.encode()) == 0
+    _, srs, geoms = _gpkg_geoms(path, "fire_references")
+    assert srs == srs_id and len(geoms) == 12
+    db = sqlite3.connect(path)
+    rows = db.execute("SELECT organization, organization_coordsys_id, definition, description "
+                      "FROM gpkg_spatial_ref_sys WHERE srs_id = ?", (srs_id,)).fetchall()
+    assert db.execute("SELECT srs_id FROM gpkg_contents").fetchone()[0] == srs_id
+    db.close()
+    assert len(rows) == 1
+    o, oid, definition, description = rows[0]
+    assert o == org and oid == srs_id
+    if srs_id != 4326:
+        assert description == crs
+    if has is None:
+        assert definition == "undefined"
+    else:
+        assert _wkt_balanced(definition)
+        for piece in has:
+            assert piece in definition, piece
+
+
 def test_boundaries_geopackage(lib, pp, tmp_path):
     """propag_write_boundaries_gpkg: the super-grid tiles ("grids") and their
     19 x 19 thread blocks ("blocks") as closed polygons (propag.rs:601-697)."""
