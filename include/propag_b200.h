@@ -13,6 +13,10 @@
  *                    cuda_standard_simple_burn) over firelib.rs:996-1188
  *   propagation      crates/propag/src/propag.cu (pre_propagate, propag,
  *                    post_propagate) driven as crates/propag/src/propag.rs:392-556
+ *   input rasters    rasterize_times / rasterize_fuels,
+ *                    crates/propag/src/propag.rs:837-890, 929-982; dead fuel
+ *                    moisture, crates/dmoist/src/lib.rs:55-137
+ *   output layers    write_refs / write_boundaries, propag.rs:576-750
  */
 #ifndef PROPAG_B200_H
 #define PROPAG_B200_H
