@@ -279,6 +279,60 @@ def test_dda_known_answers_of_the_reference(oracle, frm, to, cells):
     assert got == cells
 
 
+def _boundaries_numpy(speed, az, ecc):
+    """find_boundaries (crates/propag/src/propag.cu:345-375) restated over
+    whole arrays: a cell is a boundary when some in-grid neighbour's fire is
+    not similar to its own (similar_fires, :296-302: float differences, taken
+    in float and compared with the double thresholds 0.1 m/s, 5 degrees in
+    radians and 0.05) and the neighbour spreads faster."""
+    H, W = speed.shape
+    out = np.zeros((H, W), bool)
+    for j in (-1, 0, 1):
+        for i in (-1, 0, 1):
+            if i == 0 and j == 0:
+                continue
+            ys, xs = slice(max(0, -j), H - max(0, j)), slice(max(0, -i), W - max(0, i))
+            yn, xn = slice(max(0, j), H + min(0, j)), slice(max(0, i), W + min(0, i))
+            s_me, s_nb = speed[ys, xs], speed[yn, xn]
+            similar = ((np.abs(s_nb - s_me).astype(np.float64) < 0.1)
+                       & (np.abs(az[yn, xn] - az[ys, xs]).astype(np.float64) < 5.0 * (2 * np.pi) / 360.0)
+                       & (np.abs(ecc[yn, xn] - ecc[ys, xs]).astype(np.float64) < 0.05))
+            out[ys, xs] |= ~similar & (s_me < s_nb)
+    return out
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_find_boundaries_restated(oracle, seed):
+    """The oracle's boundary bits against the rule restated in numpy, on
+    fields drawn from lattices whose steps put many neighbour differences
+    exactly at (or one float rounding from) the thresholds, with non-burnable
+    (all-zero) cells and grids of one row or column."""
+    rng = np.random.default_rng(seed)
+    for H, W in ((17, 23), (1, 40), (31, 1), (64, 64)):
+        speed = (rng.integers(0, 8, (H, W)) * np.float32(0.05)).astype(np.float32)
+        az = (rng.integers(0, 12, (H, W)) * np.float32(2.5 * np.pi / 180)).astype(np.float32)
+        ecc = (rng.integers(0, 20, (H, W)) * np.float32(0.025)).astype(np.float32)
+        dead = rng.random((H, W)) < 0.1
+        speed[dead] = az[dead] = ecc[dead] = 0.0
+        bits = oracle.find_boundaries(W, H, speed, az, ecc)
+        got = np.unpackbits(bits.view(np.uint8), bitorder="little")[: H * W].reshape(H, W).astype(bool)
+        want = _boundaries_numpy(speed, az, ecc)
+        assert np.array_equal(got, want), (seed, H, W)
+        assert want.any() and not want.all()
+
+
+def test_find_boundaries_takes_differences_in_float(oracle):
+    """0.1f - 2e-9f is 0.09999999949 exactly, below the double 0.1, but
+    rounds to 0.1f = 0.10000000149 in float: the speeds are not similar, so
+    the slower cell is a boundary, as the reference's float subtraction
+    decides (propag.cu:296-302)."""
+    speed = np.array([[np.float32(2e-9), np.float32(0.1)]], np.float32)
+    zeros = np.zeros_like(speed)
+    bits = oracle.find_boundaries(2, 1, speed, zeros, zeros)
+    assert int(bits[0]) & 3 == 1
+    assert _boundaries_numpy(speed, zeros, zeros).tolist() == [[True, False]]
+
+
 def test_dda_special_case_propag(oracle):
     """The reference's special_case_propag: the second cell of the walk from
     (499, 99) to (500, 100) is (500, 100)."""
